@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the spectral-fluid step engine.
+
+Workload (default): the plain single-instance path at the larger size --
+a 32^3 voxel box with a solid sphere of radius 8 voxels at its centre,
+N = 128 Laplacian eigenmodes (C 128^3 and Phi stored FP32, state FP64),
+w ~ N(0, 1) with seed 2 scaled to unit energy, constant forcing of 0.1 per
+step on the lowest mode, dt = 0.005, 262,144 particles uniform in the fluid
+(seed 3) traced with RK4.  One step = contraction + state update +
+reconstruction + particle tracing for one instance.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under ``torch.distributed.run`` every rank steps its own replica (instances
+are independent; no per-step collective): weak scaling, ``value`` is the
+whole-job instance-steps/s, timed as the max over ranks of the device time.
+``--impl reference`` times the reference's CPU step (the FP64 restatement of
+Solver/SolverImpl/psfsolver.cpp:21-234; the reference itself does not build
+here) on all host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "sphere32_n128_p262144_rk4": dict(
+        domain=("sphere", 32, 8.0), n_modes=128, seed_w=2, seed_p=3, particles=262144, dt=0.005,
+        force0=0.1, integrator=4, full_steps=1000,
+        describe="32^3 box with a solid sphere of radius 8 voxels, N=128, 262144 particles, RK4, "
+                 "forcing 0.1/step on mode 0, dt=0.005"),
+    "box16_n64_p4096_rk4": dict(
+        domain=("box", 16, None), n_modes=64, seed_w=0, seed_p=1, particles=4096, dt=0.01,
+        force0=0.0, integrator=4, full_steps=100,
+        describe="16^3 all-wall box, N=64, 4096 particles, RK4, dt=0.01"),
+}
+DEFAULT_WORKLOAD = "sphere32_n128_p262144_rk4"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def make_domain(spec):
+    from parallelspectralfluids3d_b200.domain import box_domain, sphere_obstacle_domain
+
+    kind, n, r = spec
+    return sphere_obstacle_domain(n, r) if kind == "sphere" else box_domain(n)
+
+
+def load_workload(name, device):
+    from parallelspectralfluids3d_b200.fixture import cached_basis, initial_coefficients, initial_particles
+
+    wl = WORKLOADS[name]
+    b = cached_basis(make_domain(wl["domain"]), wl["n_modes"], device=device)
+    w0 = initial_coefficients(b.n_modes, wl["seed_w"])
+    parts = initial_particles(b, wl["particles"], wl["seed_p"])
+    force = np.zeros(b.n_modes)
+    force[0] = wl["force0"] / wl["dt"]
+    return wl, b, w0, parts, force
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def kernel_bytes(b, P, kind):
+    """Algorithmic bytes one launch must move (per kernel, FP32 basis)."""
+    N = b.n_modes
+    Np = (N + 3) // 4 * 4
+    Fa = b.n_active
+    if kind == "contract_state":
+        return 4 * N * N * Np + 8 * N * 3
+    if kind == "reconstruct":
+        return 4 * N * ((Fa + 3) // 4 * 4) + 4 * Fa + 4 * Fa + 8 * N
+    return 32 * P  # trace: read + write float4 per particle
+
+
+# -------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from parallelspectralfluids3d_b200 import _lib as L
+    from parallelspectralfluids3d_b200.solver import Context
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+
+    def barrier():
+        if dist:
+            td.barrier(device_ids=[local_rank])
+
+    if rank == 0:
+        wl, b, w0, parts, force = load_workload(args.workload, "cuda")
+    barrier()
+    if rank != 0:
+        wl, b, w0, parts, force = load_workload(args.workload, "cuda")
+
+    params = L.make_params(dt=wl["dt"], integrator=wl["integrator"],
+                           flags=L.PSF_FLAG_RENORM | (L.PSF_FLAG_FORCING if wl["force0"] else 0))
+    ctx = Context(b, params, device=local_rank)
+    ctx.set_forcing(force)
+    ctx.set_state(w0)
+    ctx.set_particles(parts)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    ctx.step(max(3, args.warmup))
+    ctx.sync()
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local_rank).start()
+    with torch.cuda.stream(stream):
+        for i in range(K):
+            flush.zero_()
+            starts[i].record(stream)
+            ctx.step(1)
+            ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    per_step = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    total_ms = float(per_step.sum())
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * K / (total_ms / 1e3)
+
+    # Kernel breakdown: each kernel between its own events, L2 flushed before each step.
+    M = min(K, 64)
+    names = ["contract_state", "reconstruct", "trace"][: ctx.kernels_per_step()]
+    acc = np.zeros(len(names))
+    for _ in range(M):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        acc += ctx.profile_step()
+    kms = acc / M
+    dom_i = int(np.argmax(kms))
+    peak, peak_kind = measured_peak_hbm()
+    alg = kernel_bytes(b, ctx.P, names[dom_i])
+    achieved = alg / (kms[dom_i] / 1e3) / 1e9
+    roofline = {"kernel": names[dom_i], "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "algorithmic_bytes": int(alg), "traffic": None,
+                "all_kernels": {n: {"ms": round(float(m), 5),
+                                    "GB/s": round(kernel_bytes(b, ctx.P, n) / (m / 1e3) / 1e9, 1)}
+                                for n, m in zip(names, kms)}}
+
+    # End to end through the public API: host (pinned) buffers, copies inside the region.
+    E = min(K, 50)
+    w_host = torch.from_numpy(ctx.get_state()).pin_memory()
+    p_host = torch.from_numpy(ctx.get_particles()).pin_memory()
+    w_np, p_np = w_host.numpy(), p_host.numpy()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(E):
+        ctx.set_state(w_np)
+        ctx.set_particles(p_np)
+        ctx.step(1)
+        ctx.get_state(w_np)
+        ctx.get_particles(p_np)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": round(world * E / (e2e_ms / 1e3), 2), "unit": "instance-steps/s",
+           "h2d_bytes_per_step": int(8 * b.n_modes + 16 * ctx.P),
+           "d2h_bytes_per_step": int(8 * b.n_modes + 16 * ctx.P), "steps": E}
+    ctx.close()
+
+    # Accuracy of the full configured run against the FP64 oracle, and the CPU baseline.
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        extra = accuracy_and_cpu(b, wl, w0, parts, force, params, local_rank)
+    barrier()
+
+    line = {
+        "metric": "instance-steps/s", "value": round(value, 2), "unit": "instance-steps/s",
+        "n_gpus": world, "steps": K, "warmup": max(3, args.warmup), "ms_per_step": round(total_ms / K, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "state_dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "describe": wl["describe"], "n_modes": b.n_modes,
+                   "faces_active": b.n_active, "particles": int(parts.shape[0]),
+                   "integrator": "rk4" if wl["integrator"] == 4 else "rk1", "dt": wl["dt"],
+                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+        "p50_ms": round(float(np.percentile(per_step, 50)), 5),
+        "p99_ms": round(float(np.percentile(per_step, 99)), 5),
+        "particle_steps_per_s": round(value * parts.shape[0], 1),
+        "gpu_launches": int(K * len(names)),
+        "kernel_ms": {n: round(float(m), 5) for n, m in zip(names, kms)},
+        "roofline": roofline, "e2e": e2e, "clocks": clk,
+    }
+    line.update(extra)
+    return line
+
+
+def accuracy_and_cpu(b, wl, w0, parts, force, params, device):
+    """Full configured run on the GPU vs the FP64 oracle; the oracle run is the CPU baseline."""
+    from oracle import oracle as O
+    from parallelspectralfluids3d_b200.solver import Context
+
+    S = wl["full_steps"]
+    ctx = Context(b, params, device=device)
+    ctx.set_forcing(force)
+    ctx.set_state(w0)
+    ctx.set_particles(parts)
+    ctx.step(S)
+    w_gpu = ctx.get_state()
+    p_gpu = ctx.get_particles()
+    ctx.close()
+    ref = O.OracleRollout(b, w0, parts, dt=wl["dt"], integrator=wl["integrator"], forcing=force)
+    t0 = time.perf_counter()
+    ref.step(S)
+    cpu_s = time.perf_counter() - t0
+    rel = float(np.linalg.norm(w_gpu - ref.w) / np.linalg.norm(ref.w))
+    perr = float(np.abs(p_gpu[:, :3] - ref.pos).max() / b.h)
+    return {
+        "accuracy": {"steps": S, "rel_err_w_vs_fp64": rel, "max_particle_err_voxels": perr},
+        "cpu_baseline": {"value": round(S / cpu_s, 3), "unit": "instance-steps/s", "cores": O.num_threads(),
+                         "kind": "port", "sample": f"full {S}-step run of the workload, FP64, OpenMP"},
+    }
+
+
+# -------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference's CPU step (FP64 restatement) on all host threads."""
+    from oracle import oracle as O
+
+    wl, b, w0, parts, force = load_workload(args.workload, "cpu")
+    O.build()
+    ref = O.OracleRollout(b, w0, parts, dt=wl["dt"], integrator=wl["integrator"], forcing=force)
+    ref.step(max(3, args.warmup))
+    K = args.steps
+    t0 = time.perf_counter()
+    ref.step(K)
+    dt = time.perf_counter() - t0
+    value = K / dt
+    return {
+        "impl": "reference", "metric": "instance-steps/s", "value": round(value, 3), "unit": "instance-steps/s",
+        "n_gpus": 1, "steps": K, "warmup": max(3, args.warmup), "ms_per_step": round(1e3 * dt / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "describe": wl["describe"]},
+        "cpu_baseline": {"value": round(value, 3), "unit": "instance-steps/s", "cores": O.num_threads(),
+                         "kind": "port",
+                         "sample": f"{K} steps of the full workload (reference does not build: Eigen/glm absent)"},
+        "e2e": {"value": round(value, 3), "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the FP64 accuracy/CPU baseline leg")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                              device_id=torch.device("cuda", local_rank))
+    try:
+        line = run_ours(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as td
+
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,446 @@
+// C ABI of include/psf_b200.h: single-instance contexts.
+//
+// A context replaces the reference's PSFSolverGPU host object
+// (Solver/SolverImpl/psfsolvergpu.cpp): it owns the device copies of the
+// basis, the coefficient state, the face field and the particles, one CUDA
+// stream, and a CUDA graph of one step.  Errors are returned as status codes
+// (the reference prints and calls exit(), psfsolvergpu.cpp:39-104).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "psf_b200.h"
+#include "psf_internal.h"
+
+using psf::fail;
+
+namespace {
+
+inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+int64_t n_faces_of(const psf_grid &g)
+{
+    const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
+    return (nz + 1) * nx * ny + (ny + 1) * nx * nz + (nx + 1) * ny * nz;
+}
+
+// Per-face sign with which the reference tracer reads the face velocity
+// (psfsolver.cpp:160-188): -s(v,4) / +s(v,5) for the x-faces at x / x+1 of
+// voxel v, -s(v,2) / +s(v,3) for y, +s(v,0) / -s(v,1) for z, where s is
+// DECMesh3D::getFaceSignum (DEC/decmesh3d.cpp:1848-1853).  Each face is read
+// from up to two voxels; the readings must agree for the sign to be folded.
+int fold_signs(const psf_grid &g, const uint32_t *bits, std::vector<int8_t> &sigma)
+{
+    const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
+    const int64_t yoff = (nz + 1) * nx * ny;
+    const int64_t xoff = yoff + (ny + 1) * nx * nz;
+    sigma.assign((size_t)n_faces_of(g), 0);
+    auto sgn = [&](int64_t vid, int f) -> int {
+        return ((bits[vid / 5] >> ((vid % 5) * 6 + f)) & 1u) ? 1 : -1;
+    };
+    auto put = [&](int64_t face, int s) -> bool {
+        int8_t &d = sigma[(size_t)face];
+        if (d != 0 && d != s) return false;
+        d = (int8_t)s;
+        return true;
+    };
+    for (int64_t z = 0; z < nz; ++z)
+        for (int64_t y = 0; y < ny; ++y)
+            for (int64_t x = 0; x < nx; ++x) {
+                const int64_t v = z * nx * ny + y * nx + x;
+                bool ok = put(z * ny * (nx + 1) + y * (nx + 1) + x + xoff, -sgn(v, 4)) &&
+                          put(z * ny * (nx + 1) + y * (nx + 1) + x + 1 + xoff, sgn(v, 5)) &&
+                          put(z * (ny + 1) * nx + y * nx + x + yoff, -sgn(v, 2)) &&
+                          put(z * (ny + 1) * nx + (y + 1) * nx + x + yoff, sgn(v, 3)) &&
+                          put(z * nx * ny + y * nx + x, sgn(v, 0)) &&
+                          put((z + 1) * nx * ny + y * nx + x, -sgn(v, 1));
+                if (!ok) return fail(PSF_ERR_SIGNS, "face signs of two voxels disagree; cannot fold");
+            }
+    return PSF_OK;
+}
+
+}  // namespace
+
+struct psf_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool have_state = false;
+    psf_grid grid{};
+    psf_params params{};
+    std::vector<int8_t> sigma;
+    psf::PlainDev d{};
+    std::vector<void *> allocs;
+
+    ~psf_ctx()
+    {
+        drop_graph();
+        for (void *p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void drop_graph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    template <class T>
+    int alloc(T **p, size_t count)
+    {
+        void *v = nullptr;
+        cudaError_t e = cudaMalloc(&v, std::max<size_t>(1, count) * sizeof(T));
+        if (e != cudaSuccess) return psf::cuda_fail(e, "cudaMalloc");
+        allocs.push_back(v);
+        *p = static_cast<T *>(v);
+        return PSF_OK;
+    }
+    void release(void *p)
+    {
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) {
+            cudaFree(p);
+            allocs.erase(it);
+        }
+    }
+};
+
+#define PSF_CHECK(x)                  \
+    do {                              \
+        int rc_ = (x);                \
+        if (rc_ != PSF_OK) return rc_; \
+    } while (0)
+#define PSF_CUDA(x)                                      \
+    do {                                                 \
+        cudaError_t e_ = (x);                            \
+        if (e_ != cudaSuccess) return psf::cuda_fail(e_, #x); \
+    } while (0)
+
+static int apply_params(psf_ctx *c, const psf_params &p)
+{
+    if (!(p.timestep > 0.0) || !std::isfinite(p.timestep))
+        return fail(PSF_ERR_INVALID, "timestep must be positive and finite");
+    if (p.integrator != PSF_RK1 && p.integrator != PSF_RK4)
+        return fail(PSF_ERR_INVALID, "integrator must be PSF_RK1 or PSF_RK4");
+    if (p.precision != PSF_PRECISION_FP32)
+        return fail(PSF_ERR_UNSUPPORTED, "single-instance contexts store the basis in FP32");
+    c->params = p;
+    c->d.sp.dt = p.timestep;
+    c->d.sp.visc_signed = (p.flags & PSF_FLAG_DECAY_NEG) ? -p.viscosity : p.viscosity;
+    c->d.sp.flags = p.flags;
+    c->d.tp.dt = (float)p.timestep;
+    c->d.tp.lifetime = p.lifetime;
+    c->d.tp.rk4 = p.integrator == PSF_RK4;
+    c->d.tp.seed = p.seed;
+    c->drop_graph();
+    return PSF_OK;
+}
+
+static int build_graph(psf_ctx *c)
+{
+    if (c->exec) return PSF_OK;
+    PSF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = psf::launch_contract_state(c->d, c->stream);
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->d, c->stream);
+    if (rc == PSF_OK) rc = psf::launch_trace(c->d, c->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc != PSF_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return psf::cuda_fail(e, "cudaStreamEndCapture");
+    c->graph = g;
+    PSF_CUDA(cudaGraphInstantiate(&c->exec, c->graph, 0));
+    return PSF_OK;
+}
+
+extern "C" {
+
+int psf_abi_version(void) { return PSF_ABI_VERSION; }
+
+const char *psf_last_error(void) { return psf::g_last_error.c_str(); }
+
+int psf_device_count(int *count)
+{
+    if (!count) return fail(PSF_ERR_INVALID, "count is null");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return PSF_OK;
+}
+
+int psf_create(const psf_basis_desc *b, const psf_params *params, int device, psf_ctx **out)
+{
+    if (!b || !params || !out) return fail(PSF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    const psf_grid &g = b->grid;
+    if (g.dims[0] == 0 || g.dims[1] == 0 || g.dims[2] == 0 || !(g.resolution > 0.0))
+        return fail(PSF_ERR_INVALID, "grid dims and resolution must be positive");
+    if (b->n_modes < 1 || b->n_modes > psf::PSF_MAX_MODES)
+        return fail(PSF_ERR_UNSUPPORTED, "n_modes must be in [1, 1024]");
+    if (b->n_active < 1) return fail(PSF_ERR_INVALID, "n_active must be positive");
+    if (!b->active_faces || !b->phi || !b->advection || !b->eigenvalues || !b->sign_bits)
+        return fail(PSF_ERR_INVALID, "basis arrays must not be null");
+    const int64_t F = n_faces_of(g);
+    if (F >= (int64_t)UINT32_MAX) return fail(PSF_ERR_UNSUPPORTED, "grid has too many faces");
+    for (int64_t r = 0; r < b->n_active; ++r)
+        if (b->active_faces[r] < 0 || b->active_faces[r] >= F)
+            return fail(PSF_ERR_INVALID, "active face id out of range");
+
+    psf_ctx *c = nullptr;
+    try {
+        c = new psf_ctx();
+    } catch (const std::bad_alloc &) {
+        return fail(PSF_ERR_NOMEM, "host allocation failed");
+    }
+    auto bail = [&](int rc) {
+        delete c;
+        return rc;
+    };
+    int rc = PSF_OK;
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaSetDevice"));
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaStreamCreate"));
+    c->grid = g;
+    if ((rc = fold_signs(g, b->sign_bits, c->sigma)) != PSF_OK) return bail(rc);
+
+    psf::PlainDev &d = c->d;
+    const int N = b->n_modes;
+    d.N = N;
+    d.Np = (int)round_up(N, 4);
+    d.S = std::max(1, std::min(N, (2 * c->num_sms + N - 1) / N));
+    d.n_active = b->n_active;
+    d.ldp = round_up(b->n_active, 4);
+    d.n_faces = F;
+    d.P = 0;
+
+    try {
+        // C as FP32 [k][a][j] with j padded to Np.
+        std::vector<float> hC((size_t)N * N * d.Np, 0.f);
+        for (int64_t ka = 0; ka < (int64_t)N * N; ++ka)
+            for (int j = 0; j < N; ++j) hC[(size_t)ka * d.Np + j] = (float)b->advection[(size_t)ka * N + j];
+        // Phi mode-major with the tracer's face signs folded in.
+        std::vector<float> hP((size_t)N * d.ldp, 0.f);
+        for (int64_t r = 0; r < b->n_active; ++r) {
+            const float s = (float)c->sigma[(size_t)b->active_faces[r]];
+            for (int i = 0; i < N; ++i) hP[(size_t)i * d.ldp + r] = s * (float)b->phi[(size_t)r * N + i];
+        }
+        float *C = nullptr, *phiT = nullptr;
+        int32_t *faces = nullptr;
+        double *lam = nullptr, *force = nullptr;
+        if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phiT, hP.size())) ||
+            (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&d.w, (size_t)N)) ||
+            (rc = c->alloc(&d.dwpart, (size_t)N * d.S)) || (rc = c->alloc(&lam, (size_t)N)) ||
+            (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
+            (rc = c->alloc(&d.step_ctr, 1)) || (rc = c->alloc(&d.u, (size_t)F)))
+            return bail(rc);
+        d.C = C;
+        d.phiT = phiT;
+        d.faces = faces;
+        d.lam = lam;
+        d.force = force;
+        cudaStream_t st = c->stream;
+        if ((e = cudaMemcpyAsync(C, hC.data(), hC.size() * 4, cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(phiT, hP.data(), hP.size() * 4, cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(faces, b->active_faces, (size_t)b->n_active * 4, cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(lam, b->eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemsetAsync(force, 0, (size_t)N * 8, st)) || (e = cudaMemsetAsync(d.w, 0, (size_t)N * 8, st)) ||
+            (e = cudaMemsetAsync(d.ticket, 0, 4, st)) || (e = cudaMemsetAsync(d.step_ctr, 0, 8, st)) ||
+            (e = cudaMemsetAsync(d.u, 0, (size_t)F * 4, st)) || (e = cudaStreamSynchronize(st)))
+            return bail(psf::cuda_fail(e, "basis upload"));
+    } catch (const std::bad_alloc &) {
+        return bail(fail(PSF_ERR_NOMEM, "host staging allocation failed"));
+    }
+
+    const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
+    d.grid.nx = (int)nx;
+    d.grid.ny = (int)ny;
+    d.grid.nz = (int)nz;
+    d.grid.inv_h = (float)(1.0 / g.resolution);
+    for (int q = 0; q < 3; ++q) {
+        d.grid.mn[q] = g.aabb_min[q];
+        d.grid.mx[q] = g.aabb_max[q];
+        const float ext = g.aabb_max[q] - g.aabb_min[q];
+        d.grid.shift[q] = g.aabb_min[q] + ext;
+    }
+    d.grid.yoff = (uint32_t)((nz + 1) * nx * ny);
+    d.grid.xoff = (uint32_t)((nz + 1) * nx * ny + (ny + 1) * nx * nz);
+    if ((rc = apply_params(c, *params)) != PSF_OK) return bail(rc);
+    *out = c;
+    return PSF_OK;
+}
+
+int psf_destroy(psf_ctx *c)
+{
+    if (!c) return PSF_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    delete c;
+    return PSF_OK;
+}
+
+int psf_set_params(psf_ctx *c, const psf_params *p)
+{
+    if (!c || !p) return fail(PSF_ERR_INVALID, "null argument");
+    if (p->precision != c->params.precision)
+        return fail(PSF_ERR_INVALID, "precision is fixed when the context is created");
+    return apply_params(c, *p);
+}
+
+int psf_set_state(psf_ctx *c, const double *w, int32_t n)
+{
+    if (!c || !w) return fail(PSF_ERR_INVALID, "null argument");
+    if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CUDA(cudaMemcpyAsync(c->d.w, w, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    c->have_state = true;
+    return PSF_OK;
+}
+
+int psf_get_state(psf_ctx *c, double *w, int32_t n)
+{
+    if (!c || !w) return fail(PSF_ERR_INVALID, "null argument");
+    if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CUDA(cudaMemcpyAsync(w, c->d.w, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    return PSF_OK;
+}
+
+int psf_set_forcing(psf_ctx *c, const double *f, int32_t n)
+{
+    if (!c || !f) return fail(PSF_ERR_INVALID, "null argument");
+    if (n != c->d.N) return fail(PSF_ERR_INVALID, "forcing length must equal n_modes");
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CUDA(cudaMemcpyAsync(const_cast<double *>(c->d.force), f, (size_t)n * 8, cudaMemcpyHostToDevice,
+                             c->stream));
+    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    return PSF_OK;
+}
+
+int psf_set_particles(psf_ctx *c, const float *xyzw, int64_t count)
+{
+    if (!c || (count > 0 && !xyzw)) return fail(PSF_ERR_INVALID, "null argument");
+    if (count < 0 || count > ((int64_t)1 << 31) * 64) return fail(PSF_ERR_INVALID, "bad particle count");
+    PSF_CUDA(cudaSetDevice(c->device));
+    if (count != c->d.P) {
+        PSF_CUDA(cudaStreamSynchronize(c->stream));
+        c->drop_graph();
+        if (c->d.parts) c->release(c->d.parts);
+        c->d.parts = nullptr;
+        c->d.P = 0;
+        if (count > 0) PSF_CHECK(c->alloc(&c->d.parts, (size_t)count));
+        c->d.P = count;
+    }
+    if (count > 0) {
+        PSF_CUDA(cudaMemcpyAsync(c->d.parts, xyzw, (size_t)count * 16, cudaMemcpyHostToDevice, c->stream));
+        PSF_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return PSF_OK;
+}
+
+int psf_get_particles(psf_ctx *c, float *xyzw, int64_t count)
+{
+    if (!c || (count > 0 && !xyzw)) return fail(PSF_ERR_INVALID, "null argument");
+    if (count != c->d.P) return fail(PSF_ERR_INVALID, "count must equal the number of particles");
+    if (count == 0) return PSF_OK;
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CUDA(cudaMemcpyAsync(xyzw, c->d.parts, (size_t)count * 16, cudaMemcpyDeviceToHost, c->stream));
+    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    return PSF_OK;
+}
+
+int psf_get_velocity(psf_ctx *c, float *u, int64_t n_faces)
+{
+    if (!c || !u) return fail(PSF_ERR_INVALID, "null argument");
+    if (n_faces != c->d.n_faces) return fail(PSF_ERR_INVALID, "n_faces must equal the grid's face count");
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CUDA(cudaMemcpyAsync(u, c->d.u, (size_t)n_faces * 4, cudaMemcpyDeviceToHost, c->stream));
+    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    for (int64_t f = 0; f < n_faces; ++f) u[f] *= (float)c->sigma[(size_t)f];
+    return PSF_OK;
+}
+
+int psf_step(psf_ctx *c, int32_t nsteps)
+{
+    if (!c) return fail(PSF_ERR_INVALID, "null context");
+    if (nsteps < 0) return fail(PSF_ERR_INVALID, "nsteps must be >= 0");
+    if (!c->have_state) return fail(PSF_ERR_STATE, "psf_set_state must be called before stepping");
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CHECK(build_graph(c));
+    for (int32_t i = 0; i < nsteps; ++i) PSF_CUDA(cudaGraphLaunch(c->exec, c->stream));
+    return PSF_OK;
+}
+
+int psf_sync(psf_ctx *c)
+{
+    if (!c) return fail(PSF_ERR_INVALID, "null context");
+    PSF_CUDA(cudaSetDevice(c->device));
+    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    return PSF_OK;
+}
+
+int psf_get_stream(psf_ctx *c, void **stream)
+{
+    if (!c || !stream) return fail(PSF_ERR_INVALID, "null argument");
+    *stream = (void *)c->stream;
+    return PSF_OK;
+}
+
+int psf_kernels_per_step(psf_ctx *c, int32_t *count)
+{
+    if (!c || !count) return fail(PSF_ERR_INVALID, "null argument");
+    *count = c->d.P > 0 ? 3 : 2;
+    return PSF_OK;
+}
+
+int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
+{
+    if (!c || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(PSF_ERR_STATE, "psf_set_state must be called before stepping");
+    const int nk = c->d.P > 0 ? 3 : 2;
+    if (n < nk) return fail(PSF_ERR_INVALID, "kernel_ms has fewer slots than kernels per step");
+    PSF_CUDA(cudaSetDevice(c->device));
+    cudaEvent_t ev[4];
+    for (int i = 0; i <= nk; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
+    int rc = PSF_OK;
+    cudaStream_t st = c->stream;
+    cudaEventRecord(ev[0], st);
+    if (rc == PSF_OK) rc = psf::launch_contract_state(c->d, st);
+    cudaEventRecord(ev[1], st);
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->d, st);
+    cudaEventRecord(ev[2], st);
+    if (rc == PSF_OK && nk == 3) {
+        rc = psf::launch_trace(c->d, st);
+        cudaEventRecord(ev[3], st);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");
+    for (int i = 0; rc == PSF_OK && i < nk; ++i) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        if (e != cudaSuccess) rc = psf::cuda_fail(e, "cudaEventElapsedTime");
+        kernel_ms[i] = ms;
+    }
+    for (int i = 0; i <= nk; ++i) cudaEventDestroy(ev[i]);
+    return rc;
+}
+
+}  // extern "C"

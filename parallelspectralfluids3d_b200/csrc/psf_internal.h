@@ -1,0 +1,65 @@
+// Internal types shared by the kernels and the C ABI implementation.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+namespace psf {
+
+// Largest mode count a context accepts (shared-memory staging of w).
+constexpr int PSF_MAX_MODES = 1024;
+
+// Grid constants for the tracer (DECMesh3D dims and face-block offsets,
+// DEC/decmesh3d.cpp:17-30).
+struct GridDev {
+    int nx, ny, nz;
+    float inv_h;
+    float mn[3];     // aabb min: grid origin and lower clamp
+    float mx[3];     // aabb max: upper clamp
+    float shift[3];  // aabb min + extent: the reference's index offset (psfsolver.cpp:80)
+    uint32_t yoff;   // number of z-faces
+    uint32_t xoff;   // number of z- and y-faces
+};
+
+struct StateParams {
+    double dt;
+    double visc_signed;  // +nu (CPU path) or -nu (OpenCL path)
+    unsigned int flags;
+};
+
+struct TraceParams {
+    float dt;
+    float lifetime;
+    int rk4;
+    unsigned long long seed;
+};
+
+// Device view of a single-instance context.
+struct PlainDev {
+    int N, Np, S;
+    long long n_active, ldp, n_faces, P;
+    const float *C;      // [N][N][Np]
+    const float *phiT;   // [N][ldp], signed, mode-major
+    const int32_t *faces;
+    double *w, *dwpart;
+    const double *lam, *force;
+    unsigned int *ticket;
+    unsigned long long *step_ctr;
+    float *u;            // [n_faces], signed
+    float4 *parts;
+    GridDev grid;
+    StateParams sp;
+    TraceParams tp;
+};
+
+extern thread_local std::string g_last_error;
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+int launch_contract_state(const PlainDev &d, cudaStream_t st);
+int launch_reconstruct(const PlainDev &d, cudaStream_t st);
+int launch_trace(const PlainDev &d, cudaStream_t st);
+
+}  // namespace psf

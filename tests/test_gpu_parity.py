@@ -1,0 +1,120 @@
+"""GPU path (through the C ABI) against the FP64 oracle.
+
+Tolerances: the FP32 plain path stays within 1e-5
+relative on w after 100 steps and within 1e-4 voxel on particle positions on
+the 16^3 / N = 64 workload; small domains use the same bars.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from parallelspectralfluids3d_b200 import _lib as L
+from parallelspectralfluids3d_b200.fixture import initial_coefficients, initial_particles
+from parallelspectralfluids3d_b200.solver import Context
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+W_TOL = 1e-5       # relative L2 error of w
+P_TOL_VOX = 1e-4   # max particle position error, in voxels
+U_TOL = 2e-6       # face velocity error relative to max |u|
+
+
+def run_pair(b, steps, integrator=L.PSF_RK4, dt=0.01, P=2048, seed_w=0, seed_p=1, flags=L.PSF_FLAG_RENORM,
+             visc=0.0, forcing=None, lifetime=np.inf, seed=0):
+    w0 = initial_coefficients(b.n_modes, seed_w)
+    parts = initial_particles(b, P, seed_p, lifetime=lifetime)
+    params = L.make_params(dt=dt, viscosity=visc, lifetime=lifetime, integrator=integrator, flags=flags, seed=seed)
+    ctx = Context(b, params)
+    if forcing is not None:
+        ctx.set_forcing(forcing)
+        params.flags |= L.PSF_FLAG_FORCING
+        ctx.set_params(params)
+    ctx.set_state(w0)
+    ctx.set_particles(parts)
+    ctx.step(steps)
+    ctx.sync()
+    oflags = (O.FLAG_RENORM if flags & L.PSF_FLAG_RENORM else 0) | (O.FLAG_DECAY_NEG if flags & L.PSF_FLAG_DECAY_NEG else 0)
+    ref = O.OracleRollout(b, w0, parts, dt=dt, viscosity=visc, flags=oflags, integrator=integrator,
+                          lifetime=lifetime, seed=seed, forcing=forcing)
+    ref.step(steps)
+    return ctx, ref
+
+
+@pytest.mark.parametrize("integrator", [L.PSF_RK1, L.PSF_RK4])
+def test_c1_100_steps(c1_basis, integrator):
+    ctx, ref = run_pair(c1_basis, 100, integrator=integrator, P=4096)
+    w = ctx.get_state()
+    assert rel_err(w, ref.w) <= W_TOL
+    err_vox = np.abs(ctx.get_particles()[:, :3] - ref.pos).max() / c1_basis.h
+    assert err_vox <= P_TOL_VOX
+    u = ctx.get_velocity()
+    assert np.abs(u - ref.u).max() <= U_TOL * np.abs(ref.u).max()
+
+
+@pytest.mark.parametrize("name", ["box6", "sphere10", "box576", "sphere12x10x9"])
+def test_small_domains(small_bases, name):
+    b = small_bases[name]
+    ctx, ref = run_pair(b, 25, dt=0.05, P=1000)
+    assert rel_err(ctx.get_state(), ref.w) <= W_TOL
+    assert np.abs(ctx.get_particles()[:, :3] - ref.pos).max() / b.h <= P_TOL_VOX
+
+
+def test_one_step_velocity_field_and_state(c1_basis):
+    ctx, ref = run_pair(c1_basis, 1, P=0)
+    assert rel_err(ctx.get_state(), ref.w) <= 1e-7
+    u = ctx.get_velocity()
+    assert np.abs(u - ref.u).max() <= U_TOL * np.abs(ref.u).max()
+    # Wall faces stay exactly zero.
+    mask = np.ones(c1_basis.n_faces, bool)
+    mask[c1_basis.active_faces] = False
+    assert np.all(u[mask] == 0)
+
+
+@pytest.mark.parametrize("flags", [0, L.PSF_FLAG_RENORM, L.PSF_FLAG_RENORM | L.PSF_FLAG_DECAY_NEG])
+def test_flags_viscosity_forcing(small_bases, flags):
+    b = small_bases["sphere12x10x9"]
+    f = np.zeros(b.n_modes)
+    f[0] = 0.1 / 0.02
+    ctx, ref = run_pair(b, 20, dt=0.02, P=500, flags=flags, visc=0.05, forcing=f)
+    assert rel_err(ctx.get_state(), ref.w) <= W_TOL
+
+
+def test_respawn_is_deterministic_and_matches(small_bases):
+    b = small_bases["sphere10"]
+    ctx, ref = run_pair(b, 12, dt=0.05, P=777, lifetime=4.0, seed=1234)
+    got = ctx.get_particles()
+    exp = ref.particles()
+    assert np.array_equal(got[:, 3], exp[:, 3])
+    assert np.abs(got[:, :3] - exp[:, :3]).max() / b.h <= P_TOL_VOX
+
+
+def test_graph_replay_equals_single_steps(small_bases):
+    b = small_bases["box576"]
+    w0 = initial_coefficients(b.n_modes, 9)
+    parts = initial_particles(b, 300, 9)
+    outs = []
+    for chunks in ([10], [1] * 10, [3, 7]):
+        ctx = Context(b, L.make_params(dt=0.05))
+        ctx.set_state(w0)
+        ctx.set_particles(parts)
+        for c in chunks:
+            ctx.step(c)
+        outs.append((ctx.get_state(), ctx.get_particles()))
+        ctx.close()
+    for w, p in outs[1:]:
+        assert np.array_equal(w, outs[0][0]) and np.array_equal(p, outs[0][1])
+
+
+def test_errors_are_status_codes(c1_basis):
+    ctx = Context(c1_basis, L.make_params())
+    with pytest.raises(L.PSFError) as e:
+        ctx.step(1)  # no state yet
+    assert e.value.code == -5
+    with pytest.raises(L.PSFError):
+        ctx.set_state(np.zeros(3))
+    bad = L.make_params(integrator=3)
+    with pytest.raises(L.PSFError):
+        ctx.set_params(bad)
+    ctx.close()
