@@ -169,7 +169,15 @@ def run_ours(args, rank, world, local_rank):
     ctx.set_state(w0)
     ctx.set_particles(parts)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush_w = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sink = torch.empty((), dtype=torch.float32, device=dev)
+
+    def flush_l2():
+        # Write a buffer larger than L2, then read another one: the timed kernels
+        # start from a cold L2 that holds no dirty lines of the flush itself.
+        flush_w.zero_()
+        torch.sum(flush_r, dim=0, out=sink)
 
     ctx.step(max(3, args.warmup))
     ctx.sync()
@@ -179,9 +187,14 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize(dev)
     clocks = ClockSampler(local_rank).start()
+    # Pre-roll under load so that the clock samples cover the timed region.
+    t_end = time.perf_counter() + 1.5
+    while time.perf_counter() < t_end:
+        ctx.step(50)
+        ctx.sync()
     with torch.cuda.stream(stream):
         for i in range(K):
-            flush.zero_()
+            flush_l2()
             starts[i].record(stream)
             ctx.step(1)
             ends[i].record(stream)
@@ -202,7 +215,7 @@ def run_ours(args, rank, world, local_rank):
     acc = np.zeros(len(names))
     for _ in range(M):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            flush_l2()
         acc += ctx.profile_step()
     kms = acc / M
     dom_i = int(np.argmax(kms))
@@ -258,7 +271,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": args.workload, "describe": wl["describe"], "n_modes": b.n_modes,
                    "faces_active": b.n_active, "particles": int(parts.shape[0]),
                    "integrator": "rk4" if wl["integrator"] == 4 else "rk1", "dt": wl["dt"],
-                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed before every timed step (256 MB write, then 256 MB read)", "parallelism": f"replicas x{world}"},
         "p50_ms": round(float(np.percentile(per_step, 50)), 5),
         "p99_ms": round(float(np.percentile(per_step, 99)), 5),
         "particle_steps_per_s": round(value * parts.shape[0], 1),

@@ -78,6 +78,8 @@ struct psf_ctx {
     psf_params params{};
     std::vector<int8_t> sigma;
     psf::PlainDev d{};
+    psf::OrderBufs order{};
+    int32_t *perm = nullptr;
     std::vector<void *> allocs;
 
     ~psf_ctx()
@@ -338,19 +340,40 @@ int psf_set_forcing(psf_ctx *c, const double *f, int32_t n)
 int psf_set_particles(psf_ctx *c, const float *xyzw, int64_t count)
 {
     if (!c || (count > 0 && !xyzw)) return fail(PSF_ERR_INVALID, "null argument");
-    if (count < 0 || count > ((int64_t)1 << 31) * 64) return fail(PSF_ERR_INVALID, "bad particle count");
+    if (count < 0 || count > INT32_MAX) return fail(PSF_ERR_INVALID, "bad particle count");
     PSF_CUDA(cudaSetDevice(c->device));
     if (count != c->d.P) {
         PSF_CUDA(cudaStreamSynchronize(c->stream));
         c->drop_graph();
-        if (c->d.parts) c->release(c->d.parts);
+        psf::OrderBufs &o = c->order;
+        for (void *p : {(void *)c->d.parts, (void *)c->perm, (void *)o.staging, (void *)o.keys_in,
+                        (void *)o.keys_out, (void *)o.idx_in, o.temp})
+            if (p) c->release(p);
         c->d.parts = nullptr;
+        c->perm = nullptr;
+        c->d.perm = nullptr;
+        o = psf::OrderBufs{};
         c->d.P = 0;
-        if (count > 0) PSF_CHECK(c->alloc(&c->d.parts, (size_t)count));
+        if (count > 0) {
+            size_t tmp = 0;
+            PSF_CHECK(psf::sort_particles_temp_bytes(count, &tmp));
+            unsigned char *temp = nullptr;
+            PSF_CHECK(c->alloc(&c->d.parts, (size_t)count));
+            PSF_CHECK(c->alloc(&c->perm, (size_t)count));
+            PSF_CHECK(c->alloc(&o.staging, (size_t)count));
+            PSF_CHECK(c->alloc(&o.keys_in, (size_t)count));
+            PSF_CHECK(c->alloc(&o.keys_out, (size_t)count));
+            PSF_CHECK(c->alloc(&o.idx_in, (size_t)count));
+            PSF_CHECK(c->alloc(&temp, tmp));
+            o.temp = temp;
+            o.temp_bytes = tmp;
+            c->d.perm = c->perm;
+        }
         c->d.P = count;
     }
     if (count > 0) {
-        PSF_CUDA(cudaMemcpyAsync(c->d.parts, xyzw, (size_t)count * 16, cudaMemcpyHostToDevice, c->stream));
+        PSF_CUDA(cudaMemcpyAsync(c->order.staging, xyzw, (size_t)count * 16, cudaMemcpyHostToDevice, c->stream));
+        PSF_CHECK(psf::launch_order_particles(c->d, c->order, c->stream));
         PSF_CUDA(cudaStreamSynchronize(c->stream));
     }
     return PSF_OK;
@@ -362,7 +385,8 @@ int psf_get_particles(psf_ctx *c, float *xyzw, int64_t count)
     if (count != c->d.P) return fail(PSF_ERR_INVALID, "count must equal the number of particles");
     if (count == 0) return PSF_OK;
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CUDA(cudaMemcpyAsync(xyzw, c->d.parts, (size_t)count * 16, cudaMemcpyDeviceToHost, c->stream));
+    PSF_CHECK(psf::launch_unorder_particles(c->d, c->order, c->stream));
+    PSF_CUDA(cudaMemcpyAsync(xyzw, c->order.staging, (size_t)count * 16, cudaMemcpyDeviceToHost, c->stream));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
     return PSF_OK;
 }

@@ -19,6 +19,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -292,6 +294,7 @@ __device__ __forceinline__ float3 velocity_at(const GridDev &g, const float *__r
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
 __global__ void __launch_bounds__(256) psf_trace(float4 *__restrict__ parts, long long P,
+                                                 const int32_t *__restrict__ perm,
                                                  const float *__restrict__ u, GridDev g, TraceParams tp,
                                                  const unsigned long long *__restrict__ step_ctr)
 {
@@ -327,10 +330,13 @@ __global__ void __launch_bounds__(256) psf_trace(float4 *__restrict__ parts, lon
         p.w = p.w - 1.f;
     } else {
         // psfsolver.cpp:217-222 with the counter-based generator.
+        // Particles are stored in cell order; the generator is keyed by the
+        // caller's particle index so respawns do not depend on that order.
         const uint64_t step = *step_ctr - 1ull;
-        const uint32_t r1 = respawn_hash(tp.seed, step, (uint32_t)i, 1) % 1024u;
-        const uint32_t r2 = respawn_hash(tp.seed, step, (uint32_t)i, 2) % 1024u;
-        const uint32_t r3 = respawn_hash(tp.seed, step, (uint32_t)i, 3) % 1024u;
+        const uint32_t id = (uint32_t)perm[i];
+        const uint32_t r1 = respawn_hash(tp.seed, step, id, 1) % 1024u;
+        const uint32_t r2 = respawn_hash(tp.seed, step, id, 2) % 1024u;
+        const uint32_t r3 = respawn_hash(tp.seed, step, id, 3) % 1024u;
         const float cz = g.mn[2] + 0.5f * (g.mx[2] - g.mn[2]);
         p.x = (float)(((double)r1 / 1024.0 - 0.5) * 0.25);
         p.y = g.mn[1] + 0.2f;
@@ -338,6 +344,78 @@ __global__ void __launch_bounds__(256) psf_trace(float4 *__restrict__ parts, lon
         p.w = (float)((double)tp.lifetime * ((double)r2 / 1024.0));
     }
     parts[i] = p;
+}
+
+// ------------------------------------------------------- particle order
+// Particles are kept sorted by the Morton code of their voxel so that the
+// threads of a warp gather from a few neighbouring cells of the face field.
+__device__ __forceinline__ uint32_t spread10(uint32_t v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__global__ void psf_particle_keys(const float4 *__restrict__ in, long long P, GridDev g,
+                                  uint32_t *__restrict__ keys, int32_t *__restrict__ idx)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const float4 p = in[i];
+    const int x = clampi((int)floorf((p.x - g.mn[0]) * g.inv_h), 0, g.nx - 1);
+    const int y = clampi((int)floorf((p.y - g.mn[1]) * g.inv_h), 0, g.ny - 1);
+    const int z = clampi((int)floorf((p.z - g.mn[2]) * g.inv_h), 0, g.nz - 1);
+    keys[i] = spread10((uint32_t)x) | (spread10((uint32_t)y) << 1) | (spread10((uint32_t)z) << 2);
+    idx[i] = (int32_t)i;
+}
+
+__global__ void psf_gather_particles(const float4 *__restrict__ in, const int32_t *__restrict__ perm,
+                                     float4 *__restrict__ out, long long P)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) out[i] = in[perm[i]];
+}
+
+__global__ void psf_scatter_particles(const float4 *__restrict__ in, const int32_t *__restrict__ perm,
+                                      float4 *__restrict__ out, long long P)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) out[perm[i]] = in[i];
+}
+
+int sort_particles_temp_bytes(long long P, size_t *bytes)
+{
+    *bytes = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, *bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)P);
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "cub sort sizing");
+}
+
+int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st)
+{
+    if (d.P == 0) return PSF_OK;
+    const unsigned blocks = (unsigned)((d.P + 255) / 256);
+    psf_particle_keys<<<blocks, 256, 0, st>>>(o.staging, d.P, d.grid, o.keys_in, o.idx_in);
+    size_t tmp = o.temp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(o.temp, tmp, o.keys_in, o.keys_out, o.idx_in,
+                                                    const_cast<int32_t *>(d.perm),
+                                                    (int)d.P, 0, 30, st);
+    if (e != cudaSuccess) return cuda_fail(e, "cub sort");
+    psf_gather_particles<<<blocks, 256, 0, st>>>(o.staging, d.perm, d.parts, d.P);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "particle ordering launch");
+}
+
+int launch_unorder_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st)
+{
+    if (d.P == 0) return PSF_OK;
+    const unsigned blocks = (unsigned)((d.P + 255) / 256);
+    psf_scatter_particles<<<blocks, 256, 0, st>>>(d.parts, d.perm, o.staging, d.P);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "particle un-ordering launch");
 }
 
 // ------------------------------------------------------------- launchers
@@ -379,7 +457,7 @@ int launch_trace(const PlainDev &d, cudaStream_t st)
 {
     if (d.P == 0) return PSF_OK;
     const long long blocks = (d.P + 255) / 256;
-    psf_trace<<<(unsigned)blocks, 256, 0, st>>>(d.parts, d.P, d.u, d.grid, d.tp, d.step_ctr);
+    psf_trace<<<(unsigned)blocks, 256, 0, st>>>(d.parts, d.P, d.perm, d.u, d.grid, d.tp, d.step_ctr);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_trace launch");
 }

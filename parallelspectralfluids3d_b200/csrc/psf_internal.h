@@ -48,10 +48,20 @@ struct PlainDev {
     unsigned int *ticket;
     unsigned long long *step_ctr;
     float *u;            // [n_faces], signed
-    float4 *parts;
+    float4 *parts;       // [P] in cell (Morton) order
+    const int32_t *perm; // [P] caller index of each stored particle
     GridDev grid;
     StateParams sp;
     TraceParams tp;
+};
+
+// Scratch buffers for putting particles into cell order and back.
+struct OrderBufs {
+    float4 *staging = nullptr;  // [P] caller order
+    uint32_t *keys_in = nullptr, *keys_out = nullptr;
+    int32_t *idx_in = nullptr;
+    void *temp = nullptr;
+    size_t temp_bytes = 0;
 };
 
 extern thread_local std::string g_last_error;
@@ -61,5 +71,8 @@ int cuda_fail(cudaError_t e, const char *what);
 int launch_contract_state(const PlainDev &d, cudaStream_t st);
 int launch_reconstruct(const PlainDev &d, cudaStream_t st);
 int launch_trace(const PlainDev &d, cudaStream_t st);
+int sort_particles_temp_bytes(long long P, size_t *bytes);
+int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);
+int launch_unorder_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);
 
 }  // namespace psf
