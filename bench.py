@@ -340,6 +340,27 @@ def run_reference(args):
     }
 
 
+def run_for_profiler(args):
+    """Set up the workload and launch ``args.ncu`` steps kernel by kernel (for ncu captures)."""
+    import torch
+
+    from parallelspectralfluids3d_b200 import _lib as L
+    from parallelspectralfluids3d_b200.solver import Context
+
+    wl, b, w0, parts, force = load_workload(args.workload, "cuda")
+    params = L.make_params(dt=wl["dt"], integrator=wl["integrator"],
+                           flags=L.PSF_FLAG_RENORM | (L.PSF_FLAG_FORCING if wl["force0"] else 0))
+    ctx = Context(b, params, device=0)
+    ctx.set_forcing(force)
+    ctx.set_state(w0)
+    ctx.set_particles(parts)
+    for _ in range(args.ncu):
+        ms = ctx.profile_step()
+    torch.cuda.synchronize()
+    print(json.dumps({"profiled_steps": args.ncu, "last_step_kernel_ms": [round(float(m), 5) for m in ms]}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -348,7 +369,12 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the FP64 accuracy/CPU baseline leg")
+    ap.add_argument("--ncu", type=int, default=0, metavar="S",
+                    help="profiling driver: set up the workload, then run S steps kernel by kernel and exit")
     args = ap.parse_args()
+    if args.ncu:
+        run_for_profiler(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -1,0 +1,152 @@
+// PSFSolverCUDA (include/psf/psfsolvercuda.h).
+#include "psf/psfsolvercuda.h"
+
+#include <chrono>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+PSFSolverCUDA::PSFSolverCUDA(int dev) : device(dev) { gpu = true; }
+
+PSFSolverCUDA::~PSFSolverCUDA()
+{
+    if (ctx) psf_destroy(ctx);
+}
+
+void PSFSolverCUDA::check(int rc, const char *what)
+{
+    if (rc != PSF_OK) throw std::runtime_error(std::string(what) + ": " + psf_last_error());
+}
+
+psf_params PSFSolverCUDA::params() const
+{
+    psf_params p{};
+    p.timestep = timeStep;
+    p.viscosity = viscosity;
+    p.lifetime = lifeTime;
+    p.integrator = integrator;
+    p.flags = PSF_FLAG_RENORM | (gravityActive ? PSF_FLAG_FORCING : 0u) | (decayNegative ? PSF_FLAG_DECAY_NEG : 0u);
+    p.precision = PSF_PRECISION_FP32;
+    p.seed = seed;
+    return p;
+}
+
+void PSFSolverCUDA::pushParams()
+{
+    if (!ctx) return;
+    psf_params p = params();
+    check(psf_set_params(ctx, &p), "psf_set_params");
+}
+
+void PSFSolverCUDA::buildLaplace()
+{
+    // The eigen-solve ran in the precompute; take the lowest nEigenFunctions
+    // modes (an exact prefix of the stored basis).
+    active = basis.truncated((int32_t)nEigenFunctions);
+    const size_t N = nEigenFunctions, F = (size_t)active.n_faces, Fa = active.active_faces.size();
+    eigenValues.resize(N);
+    gravity.resize(N);
+    for (size_t i = 0; i < N; ++i) {
+        eigenValues[i] = active.lam[i];
+        gravity[i] = active.gravity[i];
+    }
+    velBasisField.resize(F, N);
+    for (size_t r = 0; r < Fa; ++r)
+        for (size_t i = 0; i < N; ++i) velBasisField((size_t)active.active_faces[r], i) = active.phi[r * N + i];
+    eigenFunctions.assign(N, psf::VectorXd(F));
+    for (size_t i = 0; i < N; ++i)
+        for (size_t f = 0; f < F; ++f) eigenFunctions[i][f] = velBasisField(f, i);
+    basisCoeff = psf::VectorXd(N, 0.0);
+    velocityField = psf::VectorXf(F, 0.f);
+    forcing = gravity;
+}
+
+void PSFSolverCUDA::buildAdvection()
+{
+    if (ctx) {
+        psf_destroy(ctx);
+        ctx = nullptr;
+    }
+    psf_basis_desc d = active.desc();
+    psf_params p = params();
+    check(psf_create(&d, &p, device, &ctx), "psf_create");
+    check(psf_set_forcing(ctx, forcing.data(), (int32_t)forcing.size()), "psf_set_forcing");
+    stateChanged();
+    particlesChanged();
+}
+
+void PSFSolverCUDA::stateChanged()
+{
+    if (ctx && basisCoeff.size() == nEigenFunctions)
+        check(psf_set_state(ctx, basisCoeff.data(), (int32_t)basisCoeff.size()), "psf_set_state");
+}
+
+void PSFSolverCUDA::particlesChanged()
+{
+    if (ctx)
+        check(psf_set_particles(ctx, reinterpret_cast<const float *>(particles.data()), (int64_t)particles.size()),
+              "psf_set_particles");
+}
+
+void PSFSolverCUDA::setIntegrator(int i)
+{
+    integrator = i;
+    pushParams();
+}
+
+void PSFSolverCUDA::setDecayNegative(bool neg)
+{
+    decayNegative = neg;
+    pushParams();
+}
+
+void PSFSolverCUDA::setRespawnSeed(uint64_t s)
+{
+    seed = s;
+    pushParams();
+}
+
+void PSFSolverCUDA::setForcing(const psf::VectorXd &f)
+{
+    forcing = f;
+    if (ctx) check(psf_set_forcing(ctx, forcing.data(), (int32_t)forcing.size()), "psf_set_forcing");
+}
+
+void PSFSolverCUDA::pullState()
+{
+    check(psf_get_state(ctx, basisCoeff.data(), (int32_t)basisCoeff.size()), "psf_get_state");
+    check(psf_get_velocity(ctx, velocityField.data(), (int64_t)velocityField.size()), "psf_get_velocity");
+    check(psf_get_particles(ctx, reinterpret_cast<float *>(particles.data()), (int64_t)particles.size()),
+          "psf_get_particles");
+}
+
+void PSFSolverCUDA::integrateSteps(int n)
+{
+    if (!ctx) throw std::runtime_error("setMesh must be called before integrate");
+    check(psf_step(ctx, n), "psf_step");
+    pullState();
+    simTime += n;
+}
+
+void PSFSolverCUDA::integrate()
+{
+    // Solver/SolverImpl/psfsolvergpu.cpp:216-256: benchmark bookkeeping, one
+    // step on the device, phase times appended when benchmarking.
+    if (benchmarkFrameNo > maxFramesBenchmark) startBenchmark(false);
+    if (isBenchmark) {
+        ++benchmarkFrameNo;
+        double ms[3] = {0, 0, 0};
+        check(psf_profile_step(ctx, ms, 3), "psf_profile_step");
+        benchmarkSums[0] += ms[0] + ms[1];  // coefficient update + reconstruction
+        benchmarkSums[1] += ms[2];          // particles
+        pullState();
+        simTime += 1.0;
+        return;
+    }
+    integrateSteps(1);
+}
+
+void PSFSolverCUDA::drawParticles(ShaderProgram *, const glm::mat4 &)
+{
+    // Rendering is outside the headless build; particles are read with getParticles().
+}
