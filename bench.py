@@ -48,6 +48,14 @@ WORKLOADS = {
 DEFAULT_WORKLOAD = "sphere32_n128_p262144_rk4"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
+# DRAM bytes (read + write) per launch from one ncu capture of each kernel on
+# the named workload (profiles/step_kernels_sphere32_n128_p262144_rk4.md).
+NCU_TRAFFIC = {
+    ("sphere32_n128_p262144_rk4", "contract_state"): 8410880,
+    ("sphere32_n128_p262144_rk4", "reconstruct"): 45458432 + 1024,
+    ("sphere32_n128_p262144_rk4", "trace"): 4623104,
+}
+
 
 def make_domain(spec):
     from parallelspectralfluids3d_b200.domain import box_domain, sphere_obstacle_domain
@@ -227,7 +235,8 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg / (kms[dom_i] / 1e3) / 1e9
     roofline = {"kernel": names[dom_i], "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "algorithmic_bytes": int(alg), "traffic": None,
+                "algorithmic_bytes": int(alg),
+                "traffic": NCU_TRAFFIC.get((args.workload, names[dom_i])),
                 "all_kernels": {n: {"ms": round(float(m), 5),
                                     "GB/s": round(kernel_bytes(b, ctx.P, n) / (m / 1e3) / 1e9, 1)}
                                 for n, m in zip(names, kms)}}

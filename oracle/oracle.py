@@ -4,6 +4,9 @@ Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline
 legs use this module.  It builds ``oracle/libpsf_oracle.so`` from
 ``oracle/psf_oracle.c`` and runs the reference's step semantics
 (Solver/SolverImpl/psfsolver.cpp:21-234) on a basis.
+
+Parity unpinned: the reference has no tests or golden vectors for this path
+and does not build here (Eigen3, glm, OpenCL, Qt absent).
 """
 
 from __future__ import annotations

@@ -20,6 +20,11 @@
  * clamped to the box like the final one), the GPU kernel's decay sign
  * exp(-nu lam dt) (Resources/Simulation/simulation.cl:211), and a
  * deterministic counter-based respawn generator in place of rand().
+ *
+ * Parity unpinned: the reference ships no tests, golden vectors or fixtures
+ * for this path and cannot be compiled here (Eigen3, glm, OpenCL and Qt are
+ * absent), so this restatement is checked against independent NumPy
+ * restatements and known answers only.
  */
 #include <math.h>
 #include <stdint.h>
