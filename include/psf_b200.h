@@ -159,6 +159,38 @@ int psf_kernels_per_step(psf_ctx *ctx, int32_t *count);
  */
 int psf_profile_step(psf_ctx *ctx, double *kernel_ms, int32_t n);
 
+/*
+ * Allocation-free coefficient step.  No counterpart in the reference: it is
+ * for hosts that cannot let a library call cudaMalloc -- a real-time frame
+ * loop that cannot take the device-wide stall an allocation may cause, or an
+ * embedding application that owns all device memory in its own pool and only
+ * passes device pointers.
+ *
+ * Runs one contraction + FP64 state update (the coefficient half of
+ * psf_step: psfsolver.cpp:34-59) on the caller's device buffers, enqueued on
+ * `stream` (a cudaStream_t, 0 for the legacy default stream) of the current
+ * device:
+ *   advection_f32  device, FP32 [N][N][Np] with Np = round_up(N, 4),
+ *                  C[k][a][j] at (k * N + a) * Np + j, padding ignored
+ *   w              device, FP64 [N], read and overwritten with the new state
+ *   eigenvalues    device, FP64 [N]
+ *   forcing        device, FP64 [N]; may be NULL unless PSF_FLAG_FORCING
+ *   params         host; timestep, viscosity and flags are used
+ * The kernel's scratch lives in a fixed array of PSF_STATIC_SCRATCH_BYTES in
+ * the library's device data, held by every GPU that loads the library until
+ * the process exits.  N is limited to PSF_STATIC_MAX_MODES (larger sizes
+ * return PSF_ERR_UNSUPPORTED).  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress) with the device current;
+ * make that first call before any stream capture.  The function never calls
+ * cudaMalloc or cudaFree.  All calls share the one array: calls whose
+ * kernels may overlap on the GPU (unordered streams or threads) race and
+ * corrupt each other's results, so order them on one stream.
+ */
+#define PSF_STATIC_MAX_MODES 1024
+#define PSF_STATIC_SCRATCH_BYTES (4096 * 8 + 128)
+int psf_coeff_step_static(const float *advection_f32, int32_t n_modes, double *w, const double *eigenvalues,
+                          const double *forcing, const psf_params *params, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,7 +79,7 @@ EXPORTS = (
     "psf_abi_version", "psf_last_error", "psf_device_count", "psf_create", "psf_destroy",
     "psf_set_params", "psf_set_state", "psf_get_state", "psf_set_forcing", "psf_set_particles",
     "psf_get_particles", "psf_get_velocity", "psf_step", "psf_sync", "psf_get_stream",
-    "psf_kernels_per_step", "psf_profile_step",
+    "psf_kernels_per_step", "psf_profile_step", "psf_coeff_step_static",
 )
 
 _lib = None
@@ -114,6 +114,7 @@ def load(path: str | None = None):
     L.psf_get_stream.argtypes = [vp, ct.POINTER(vp)]
     L.psf_kernels_per_step.argtypes = [vp, ct.POINTER(ct.c_int32)]
     L.psf_profile_step.argtypes = [vp, ct.POINTER(ct.c_double), ct.c_int32]
+    L.psf_coeff_step_static.argtypes = [vp, ct.c_int32, vp, vp, vp, ct.POINTER(Params), vp]
     _extend(L)
     _lib = L
     return L
