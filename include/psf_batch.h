@@ -1,0 +1,103 @@
+/*
+ * psf_batch.h -- C ABI of the batched (many-instance) spectral-fluid engine.
+ *
+ * The reference steps one instance per solver object
+ * (AbstractSolver::integrate, Solver/abstractsolver.h:18; one OpenCL queue,
+ * Solver/SolverImpl/psfsolvergpu.cpp:216-256).  A batch steps many instances
+ * ("slots") at once: every slot of a basis shares that basis' C and Phi,
+ * which are read once per step by tensor-core GEMMs whose narrow operand is
+ * the slots' coefficient vectors.  Slots may use fewer modes than their basis
+ * (a prefix slice, zero-padded exactly), and have their own dt, viscosity,
+ * flags, integrator, forcing, state and particles.
+ *
+ * Precision (PSF_PRECISION_BF16X2): C and Phi are stored as BF16 hi + lo
+ * pairs, the state as BF16 hi + lo for the products, each product is
+ * compensated (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the state
+ * update and the energy renormalisation are FP64.
+ *
+ * Conventions as in psf_b200.h: int status returns, host buffers owned by
+ * the caller, one CUDA stream per batch, not thread-safe.
+ */
+#ifndef PSF_BATCH_H
+#define PSF_BATCH_H
+
+#include "psf_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSF_BATCH_MAX_BASES 6
+#define PSF_BATCH_MAX_SLOTS 256
+
+/* One basis of a batch and the slots it serves. */
+typedef struct psf_batch_basis {
+    psf_basis_desc basis;     /* host arrays, read during psf_batch_create */
+    int32_t slots;            /* instance slots on this basis, 1..PSF_BATCH_MAX_SLOTS */
+    int64_t max_particles;    /* particle capacity of each slot */
+} psf_batch_basis;
+
+typedef struct psf_batch_config {
+    int32_t n_bases;                 /* 1..PSF_BATCH_MAX_BASES */
+    const psf_batch_basis *bases;
+    int32_t precision;               /* PSF_PRECISION_BF16X2 */
+    int32_t autotune;                /* 1: time the kernel variants at creation and keep the fastest */
+    int32_t gemm_columns;            /* 0, or force the GEMM variant: 64, 128 or 256 */
+    int32_t gemm_ctas;               /* 0 (one per SM), or force the persistent grid size */
+} psf_batch_config;
+
+/* One instance placed in a slot. */
+typedef struct psf_instance_desc {
+    int32_t n_modes;          /* <= the basis' n_modes: the lowest n_modes modes */
+    psf_params params;        /* timestep, viscosity, lifetime, integrator, flags, seed */
+    const double *w0;         /* [n_modes] initial coefficients */
+    const double *forcing;    /* [n_modes] or NULL */
+    const float *particles;   /* [n_particles][4] (x, y, z, life) or NULL */
+    int64_t n_particles;      /* <= the basis' max_particles */
+} psf_instance_desc;
+
+typedef struct psf_batch psf_batch;
+
+/* Kernel variant the batch runs (chosen by the autotuner or forced). */
+typedef struct psf_batch_info {
+    int32_t gemm_columns;      /* MMA N capacity per accumulator: 64, 128 or 256 */
+    int32_t gemm_ctas;         /* persistent CTAs of the GEMM kernels */
+    int32_t trace_ctas;        /* persistent CTAs of the tracer */
+    int32_t kernels_per_step;  /* launches per psf_batch_step(b, 1) */
+    int64_t device_bytes;      /* device memory held by the batch */
+    double tuned_ms;           /* GEMM time of the chosen variant at tuning (0 if not tuned) */
+} psf_batch_info;
+
+int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out);
+int psf_batch_destroy(psf_batch *b);
+int psf_batch_info_get(psf_batch *b, psf_batch_info *info);
+
+/* Place an instance in slot `slot` of basis `basis` (replaces what was there),
+ * or empty the slot.  Ordered on the batch stream; returns when done. */
+int psf_batch_set_instance(psf_batch *b, int32_t basis, int32_t slot, const psf_instance_desc *inst);
+int psf_batch_clear_instance(psf_batch *b, int32_t basis, int32_t slot);
+
+/* Enqueue `nsteps` steps of every occupied slot (asynchronous, graph replay). */
+int psf_batch_step(psf_batch *b, int32_t nsteps);
+int psf_batch_sync(psf_batch *b);
+int psf_batch_get_stream(psf_batch *b, void **stream);
+
+/* Per-slot results (synchronising). */
+int psf_batch_get_state(psf_batch *b, int32_t basis, int32_t slot, double *w, int32_t n);
+int psf_batch_get_particles(psf_batch *b, int32_t basis, int32_t slot, float *xyzw, int64_t count);
+int psf_batch_get_velocity(psf_batch *b, int32_t basis, int32_t slot, float *u, int64_t n_faces);
+int psf_batch_get_steps(psf_batch *b, int32_t basis, int32_t slot, int64_t *steps);
+
+/* One step with each kernel timed between CUDA events (milliseconds, launch
+ * order: contraction GEMM, state update, reconstruction GEMM, tracer). */
+int psf_batch_profile_step(psf_batch *b, double *kernel_ms, int32_t n);
+
+/* Device error word of the tensor-core kernels: 0, or the code of a bounded
+ * wait that gave up (the batch must then be destroyed). */
+int psf_batch_device_status(psf_batch *b, int32_t *code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSF_BATCH_H */

@@ -45,7 +45,7 @@ def _stale(target, deps) -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     srcs = _sources()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
-    headers += [os.path.join(INCLUDE, "psf_b200.h")]
+    headers += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     headers += [os.path.join(INCLUDE, "psf", f) for f in os.listdir(os.path.join(INCLUDE, "psf"))]
     if force or _stale(LIB, srcs + headers):
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",

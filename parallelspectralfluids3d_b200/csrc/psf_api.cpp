@@ -24,6 +24,10 @@ namespace {
 
 inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+}  // namespace
+
+namespace psf {
+
 int64_t n_faces_of(const psf_grid &g)
 {
     const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
@@ -65,7 +69,29 @@ int fold_signs(const psf_grid &g, const uint32_t *bits, std::vector<int8_t> &sig
     return PSF_OK;
 }
 
-}  // namespace
+psf::GridDev make_grid_dev(const psf_grid &g)
+{
+    GridDev d{};
+    const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
+    d.nx = (int)nx;
+    d.ny = (int)ny;
+    d.nz = (int)nz;
+    d.inv_h = (float)(1.0 / g.resolution);
+    for (int q = 0; q < 3; ++q) {
+        d.mn[q] = g.aabb_min[q];
+        d.mx[q] = g.aabb_max[q];
+        const float ext = g.aabb_max[q] - g.aabb_min[q];
+        d.shift[q] = g.aabb_min[q] + ext;
+    }
+    d.yoff = (uint32_t)((nz + 1) * nx * ny);
+    d.xoff = (uint32_t)((nz + 1) * nx * ny + (ny + 1) * nx * nz);
+    return d;
+}
+
+}  // namespace psf
+
+using psf::fold_signs;
+using psf::n_faces_of;
 
 struct psf_ctx {
     int device = 0;
@@ -270,19 +296,7 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         return bail(fail(PSF_ERR_NOMEM, "host staging allocation failed"));
     }
 
-    const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
-    d.grid.nx = (int)nx;
-    d.grid.ny = (int)ny;
-    d.grid.nz = (int)nz;
-    d.grid.inv_h = (float)(1.0 / g.resolution);
-    for (int q = 0; q < 3; ++q) {
-        d.grid.mn[q] = g.aabb_min[q];
-        d.grid.mx[q] = g.aabb_max[q];
-        const float ext = g.aabb_max[q] - g.aabb_min[q];
-        d.grid.shift[q] = g.aabb_min[q] + ext;
-    }
-    d.grid.yoff = (uint32_t)((nz + 1) * nx * ny);
-    d.grid.xoff = (uint32_t)((nz + 1) * nx * ny + (ny + 1) * nx * nz);
+    d.grid = psf::make_grid_dev(g);
     if ((rc = apply_params(c, *params)) != PSF_OK) return bail(rc);
     *out = c;
     return PSF_OK;

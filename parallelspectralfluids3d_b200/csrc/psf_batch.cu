@@ -1,0 +1,484 @@
+// Batched spectral-fluid step on the 5th-generation tensor cores (sm_100a).
+//
+// Many instances ("slots") share one domain basis; a batch may hold several
+// bases.  For the slots of one basis the two dense products of a step are
+// GEMMs with the slots' coefficient vectors as the narrow operand:
+//
+//   contraction     Y[(k,a), b] = sum_j C[k][a][j] W[j][b]     (M = N*N, K = N)
+//                   dw[k][b]    = sum_a w[a][b] Y[(k,a), b]     (epilogue, FP64)
+//   reconstruction  U[f, b]     = sum_i Phi[f][i] W[i][b]       (M = F_act, K = N)
+//
+// C, Phi and W are stored as BF16 hi + lo pairs (x = hi + lo with both parts
+// rounded to nearest) and each product is compensated:
+// A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32 in TMEM.  Slots with
+// fewer modes than the basis are zero-padded, which is exact: their W rows
+// beyond N_b are zero, and dw_k for k >= N_b is ignored.
+//
+// psf_batch_gemm is one persistent kernel per GEMM over the tiles of every
+// basis: warp 0 streams 128-row A tiles and the W tile through a TMA ring of
+// shared-memory stages (128-byte swizzle, no multicast), warp 1 issues the
+// tcgen05.mma chain for a tile into one of two TMEM accumulators, warps 2-5
+// drain the other accumulator (tcgen05.ld) and run the epilogue, so loads,
+// MMAs and epilogue overlap.  The FP64 state update of every slot
+// (psf_batch_state) and the tracer (psf_batch_trace, the same interpolant as
+// the single-instance path) complete the step.
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+
+#include "psf_b200.h"
+#include "psf_batch_internal.h"
+#include "psf_device.cuh"
+#include "psf_internal.h"
+#include "psf_sm100.cuh"
+
+namespace psf {
+
+using namespace sm100;
+
+template <int BN_MAX>
+struct GemmCfg {
+    static constexpr int STAGES = BN_MAX == 64 ? 4 : (BN_MAX == 128 ? 3 : 2);
+    static constexpr int A_BYTES = 2 * 128 * 128;  // hi + lo: 128 rows x 64 BF16
+    static constexpr int B_BYTES = 2 * BN_MAX * 128;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+    static constexpr int TMEM_COLS = 2 * BN_MAX;   // two accumulators
+    static constexpr int BAR_BYTES = 256;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + BAR_BYTES + 1024;  // + alignment slack
+};
+
+__device__ __forceinline__ int find_group(const GemmArgs &args, int t, int *local)
+{
+    int g = 0;
+    while (g + 1 < args.n_groups && t >= args.g[g].tiles) {
+        t -= args.g[g].tiles;
+        ++g;
+    }
+    *local = t;
+    return g;
+}
+
+// 32 values per lane -> lane l holds the sum over the warp of value l.
+__device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lane)
+{
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = (lane & s) != 0;
+#pragma unroll
+        for (int i = 0; i < s; ++i) {
+            const double send = upper ? v[i] : v[i + s];
+            const double keep = upper ? v[i + s] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+        }
+    }
+    return v[0];
+}
+
+template <int BN_MAX, int EPI>
+__global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_constant__ GemmArgs args)
+{
+    using Cfg = GemmCfg<BN_MAX>;
+    constexpr int STAGES = Cfg::STAGES;
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw_addr = smem_u32(smem_raw);
+    unsigned char *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * Cfg::STAGE_BYTES);
+    uint64_t *full = bars;
+    uint64_t *empty = bars + STAGES;
+    uint64_t *acc_full = bars + 2 * STAGES;
+    uint64_t *acc_empty = acc_full + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *err = args.err;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 128);
+        }
+        mbar_fence_init();
+        for (int g = 0; g < args.n_groups; ++g) {
+            tma_prefetch_desc(&args.g[g].tmA);
+            tma_prefetch_desc(&args.g[g].tmB);
+        }
+    }
+    if (warp == 1) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------------------------------------------- TMA producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t last_parity[STAGES];
+            bool issued[STAGES];
+            for (int s = 0; s < STAGES; ++s) issued[s] = false;
+            bool ok = true;
+            for (int t = blockIdx.x; ok && t < args.total_tiles; t += gridDim.x) {
+                int lt;
+                const GemmGroup &G = args.g[find_group(args, t, &lt)];
+                const int outer = lt / G.m_inner, inner = lt - outer * G.m_inner;
+                for (int kc = 0; kc < G.k_chunks; ++kc) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1u, err, ERR_WAIT_EMPTY)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *sA = smem + stage * Cfg::STAGE_BYTES;
+                    unsigned char *sB = sA + Cfg::A_BYTES;
+                    mbar_arrive_expect_tx(&full[stage], G.tx_bytes);
+                    tma_load_4d(sA, &G.tmA, &full[stage], kc * 64, inner * 128, 0, outer);
+                    tma_load_3d(sB, &G.tmB, &full[stage], kc * 64, 0, 0);
+                    issued[stage] = true;
+                    last_parity[stage] = phase;
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            // After an error elsewhere, copies may still be in flight that no
+            // one consumes: wait (bounded) for them before the CTA exits.
+            if (*(volatile int *)err != 0)
+                for (int s = 0; s < STAGES; ++s)
+                    if (issued[s]) mbar_wait(&full[s], last_parity[s], err, ERR_WAIT_DRAIN);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int abuf = 0;
+            uint32_t aphase = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; ok && t < args.total_tiles; t += gridDim.x) {
+                int lt;
+                const GemmGroup &G = args.g[find_group(args, t, &lt)];
+                if (!mbar_wait(&acc_empty[abuf], aphase ^ 1u, err, ERR_WAIT_ACC_EMPTY)) break;
+                tc_fence_after();
+                const uint32_t d = tmem_base + (uint32_t)(abuf * BN_MAX);
+                const uint32_t idesc = idesc_bf16_f32(128, G.bn);
+                for (int kc = 0; kc < G.k_chunks; ++kc) {
+                    if (!mbar_wait(&full[stage], phase, err, ERR_WAIT_FULL)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(smem + stage * Cfg::STAGE_BYTES);
+                    const uint32_t b0 = a0 + Cfg::A_BYTES;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint64_t ah = desc_kmajor_sw128(a0 + kk * 32);
+                        const uint64_t al = desc_kmajor_sw128(a0 + 128 * 128 + kk * 32);
+                        const uint64_t bh = desc_kmajor_sw128(b0 + kk * 32);
+                        const uint64_t bl = desc_kmajor_sw128(b0 + (uint32_t)G.bn * 128u + kk * 32);
+                        mma_bf16(d, ah, bh, idesc, (kc | kk) ? 1u : 0u);
+                        mma_bf16(d, ah, bl, idesc, 1u);
+                        mma_bf16(d, al, bh, idesc, 1u);
+                    }
+                    mma_commit(&empty[stage]);
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[abuf]);
+                if (++abuf == 2) {
+                    abuf = 0;
+                    aphase ^= 1u;
+                }
+            }
+        }
+    } else {
+        // -------------------------------------------------------- epilogue
+        const int q = warp & 3;  // TMEM lanes 32q .. 32q+31 belong to this warp
+        const int row = q * 32 + lane;
+        int abuf = 0;
+        uint32_t aphase = 0;
+        for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
+            int lt;
+            const GemmGroup &G = args.g[find_group(args, t, &lt)];
+            const int outer = lt / G.m_inner, inner = lt - outer * G.m_inner;
+            bool ok = mbar_wait(&acc_full[abuf], aphase, err, ERR_WAIT_ACC_FULL);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * BN_MAX);
+            if (EPI == 0) {
+                // dw partial of mode k = outer over this warp's 32 rows a.
+                const int a = inner * 128 + row;
+                const bool arow = a < G.n_rows;
+                for (int c0 = 0; c0 < G.bn; c0 += 32) {
+                    float y[32];
+                    tmem_ld32(tbase + (uint32_t)c0, y);
+                    double v[32];
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        const int b = c0 + c;
+                        v[c] = (arow && b < G.cap) ? (double)y[c] * __ldg(G.w + (size_t)b * G.ldw + a) : 0.0;
+                    }
+                    const double s = warp_reduce_scatter32(v, lane);
+                    const int b = c0 + lane;
+                    if (b < G.cap)
+                        G.dwpart[((size_t)(outer * G.m_inner + inner) * 4 + q) * G.cap + b] = s;
+                }
+            } else {
+                // Face velocities of this warp's 32 rows, scattered to the
+                // reference face numbering of every slot's field.
+                const long long f = (long long)inner * 128 + row;
+                const bool frow = f < G.n_rows;
+                const long long face = frow ? (long long)__ldg(G.faces + f) : 0;
+                for (int c0 = 0; c0 < G.bn; c0 += 32) {
+                    float y[32];
+                    tmem_ld32(tbase + (uint32_t)c0, y);
+                    if (frow) {
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            const int b = c0 + c;
+                            if (b < G.cap) G.u[(size_t)b * G.n_faces + face] = y[c];
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[abuf]);
+            if (++abuf == 2) {
+                abuf = 0;
+                aphase ^= 1u;
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------ state update
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *hi, __nv_bfloat16 *lo)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    *hi = h;
+    *lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+}
+
+// FP64 update of one slot in the reference's order (psfsolver.cpp:37-59),
+// then the new state's BF16 hi/lo split for the next products.
+__global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restrict__ groups,
+                                                       SlotDev *__restrict__ slots)
+{
+    __shared__ double red[8];
+    __shared__ double wnew[PSF_MAX_MODES];
+    SlotDev &s = slots[blockIdx.x];
+    if (!s.active) return;
+    const GroupDev &G = groups[s.group];
+    const int b = s.slot, N = s.n_modes, at = G.a_tiles, cap = G.cap;
+    double *w = G.w + (size_t)b * G.N;
+    double e1 = 0.0, e2 = 0.0;
+    for (int i = threadIdx.x; i < N; i += 256) {
+        double dw = 0.0;
+        for (int t = 0; t < at; ++t)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dw += G.dwpart[((size_t)(i * at + t) * 4 + q) * cap + b];
+        const double wi = w[i];
+        const double w1 = wi + s.dt * dw;
+        wnew[i] = w1;
+        e1 += wi * wi;
+        e2 += w1 * w1;
+    }
+    e1 = block_sum_256(e1, red);
+    e2 = block_sum_256(e2, red);
+    const double scale = (s.flags & PSF_FLAG_RENORM) ? sqrt(e1 / e2) : 1.0;
+    __nv_bfloat16 *Whi = reinterpret_cast<__nv_bfloat16 *>(G.W) + (size_t)b * G.Nj;
+    __nv_bfloat16 *Wlo = Whi + (size_t)G.bn * G.Nj;
+    for (int i = threadIdx.x; i < N; i += 256) {
+        double v = wnew[i] * scale;
+        v *= exp(s.visc_signed * G.lam[i] * s.dt);
+        if (s.flags & PSF_FLAG_FORCING) v += s.dt * G.force[(size_t)b * G.N + i];
+        w[i] = v;
+        split_bf16(v, Whi + i, Wlo + i);
+    }
+    if (threadIdx.x == 0) s.step += 1ull;
+}
+
+// BF16 split of one slot's current state (after it was set from the host).
+__global__ void psf_batch_pack(const GroupDev *__restrict__ groups, const SlotDev *__restrict__ slots, int sg)
+{
+    const SlotDev &s = slots[sg];
+    const GroupDev &G = groups[s.group];
+    __nv_bfloat16 *Whi = reinterpret_cast<__nv_bfloat16 *>(G.W) + (size_t)s.slot * G.Nj;
+    __nv_bfloat16 *Wlo = Whi + (size_t)G.bn * G.Nj;
+    for (int i = threadIdx.x; i < G.Nj; i += blockDim.x) {
+        const double v = (s.active && i < s.n_modes) ? G.w[(size_t)s.slot * G.N + i] : 0.0;
+        split_bf16(v, Whi + i, Wlo + i);
+    }
+}
+
+// ------------------------------------------------------------------ tracer
+__global__ void __launch_bounds__(256) psf_batch_trace(const GroupDev *__restrict__ groups,
+                                                       const SlotDev *__restrict__ slots,
+                                                       const TraceItem *__restrict__ items,
+                                                       const int *__restrict__ n_items)
+{
+    const int n = *n_items;
+    for (int it = blockIdx.x; it < n; it += gridDim.x) {
+        const TraceItem ti = items[it];
+        if ((int)threadIdx.x >= ti.count) continue;
+        const SlotDev &s = slots[ti.slot_global];
+        const GroupDev &G = groups[s.group];
+        const size_t idx = (size_t)s.slot * (size_t)G.pmax + (size_t)ti.start + threadIdx.x;
+        TraceParams tp;
+        tp.dt = (float)s.dt;
+        tp.lifetime = s.lifetime;
+        tp.rk4 = s.rk4;
+        tp.seed = s.seed;
+        float4 p = G.parts[idx];
+        p = advance_particle(p, G.grid, G.u + (size_t)s.slot * (size_t)G.n_faces, tp, s.step - 1ull,
+                             (uint32_t)G.perm[idx]);
+        G.parts[idx] = p;
+    }
+}
+
+// --------------------------------------------------------------- launchers
+int batch_gemm_smem_bytes(int bn_max)
+{
+    switch (bn_max) {
+    case 64: return GemmCfg<64>::SMEM;
+    case 128: return GemmCfg<128>::SMEM;
+    case 256: return GemmCfg<256>::SMEM;
+    default: return -1;
+    }
+}
+
+template <int BN, int EPI>
+static int launch_gemm_t(const GemmArgs &args, int grid, cudaStream_t st)
+{
+    // The shared-memory limit is a per-device attribute of the kernel.
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured & bit)) {
+        e = cudaFuncSetAttribute(psf_batch_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 GemmCfg<BN>::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(psf_batch_gemm)");
+        configured |= bit;
+    }
+    psf_batch_gemm<BN, EPI><<<grid, GEMM_THREADS, GemmCfg<BN>::SMEM, st>>>(args);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_batch_gemm launch");
+}
+
+int launch_batch_gemm(const GemmArgs &args, int epilogue, int bn_max, int grid, cudaStream_t st)
+{
+    if (args.total_tiles <= 0) return PSF_OK;
+    grid = std::max(1, std::min(grid, args.total_tiles));
+    for (int g = 0; g < args.n_groups; ++g)
+        if (args.g[g].bn > bn_max || args.g[g].bn % 16 != 0 || args.g[g].bn < 16)
+            return fail(PSF_ERR_INVALID, "GEMM group N tile does not fit the kernel variant");
+    if (epilogue == 0) {
+        switch (bn_max) {
+        case 64: return launch_gemm_t<64, 0>(args, grid, st);
+        case 128: return launch_gemm_t<128, 0>(args, grid, st);
+        case 256: return launch_gemm_t<256, 0>(args, grid, st);
+        }
+    } else {
+        switch (bn_max) {
+        case 64: return launch_gemm_t<64, 1>(args, grid, st);
+        case 128: return launch_gemm_t<128, 1>(args, grid, st);
+        case 256: return launch_gemm_t<256, 1>(args, grid, st);
+        }
+    }
+    return fail(PSF_ERR_UNSUPPORTED, "GEMM variant must have 64, 128 or 256 columns");
+}
+
+int launch_batch_state(const GroupDev *groups, SlotDev *slots, int n_slots, cudaStream_t st)
+{
+    if (n_slots <= 0) return PSF_OK;
+    psf_batch_state<<<n_slots, 256, 0, st>>>(groups, slots);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_batch_state launch");
+}
+
+int launch_batch_pack(const GroupDev *groups, const SlotDev *slots, int slot_global, cudaStream_t st)
+{
+    psf_batch_pack<<<1, 256, 0, st>>>(groups, slots, slot_global);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_batch_pack launch");
+}
+
+int batch_trace_grid(int num_sms)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_trace, 256, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 4;
+    return num_sms * per_sm;
+}
+
+int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const TraceItem *items, const int *n_items,
+                       int grid, cudaStream_t st)
+{
+    psf_batch_trace<<<grid, 256, 0, st>>>(groups, slots, items, n_items);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_batch_trace launch");
+}
+
+// ------------------------------------------------------------ host helpers
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_tensor_map(CUtensorMap *map, void *base, int rank, const uint64_t *dims, const uint64_t *strides_bytes,
+                      const uint32_t *box)
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+            return fail(PSF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    cuuint64_t d[5];
+    cuuint64_t s[4];
+    cuuint32_t bx[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        d[i] = dims[i];
+        bx[i] = box[i];
+        es[i] = 1;
+        if (i + 1 < rank) s[i] = strides_bytes[i];
+    }
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, base, d, s, bx, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PSF_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
+    return PSF_OK;
+}
+
+void split_bf16_host(double x, uint16_t *hi, uint16_t *lo)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    const __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+    std::memcpy(hi, &h, 2);
+    std::memcpy(lo, &l, 2);
+}
+
+}  // namespace psf

@@ -1,0 +1,724 @@
+// C ABI of include/psf_batch.h: the batched engine.
+//
+// A batch owns, per basis, the BF16 hi/lo copies of C and Phi laid out for
+// TMA (K-major rows of 64 elements, 128-byte swizzle), the slots' FP64 state
+// and forcing, the BF16 hi/lo copy of the state used as the GEMMs' narrow
+// operand, the partial sums of the contraction, the slots' face fields and
+// particles; plus device tables of slots and tracer work items, so that one
+// captured CUDA graph serves every occupancy of the slots.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "psf_b200.h"
+#include "psf_batch.h"
+#include "psf_batch_internal.h"
+#include "psf_internal.h"
+
+using psf::fail;
+
+namespace {
+
+inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+#define PSF_CHECK(x)                   \
+    do {                               \
+        int rc_ = (x);                 \
+        if (rc_ != PSF_OK) return rc_; \
+    } while (0)
+#define PSF_CUDA(x)                                           \
+    do {                                                      \
+        cudaError_t e_ = (x);                                 \
+        if (e_ != cudaSuccess) return psf::cuda_fail(e_, #x); \
+    } while (0)
+
+struct HostGroup {
+    int N = 0, Nj = 0, Na = 0, a_tiles = 0;
+    int cap = 0, bn = 0, slot_base = 0;
+    int64_t F_act = 0, Fp = 0, n_faces = 0, pmax = 0;
+    psf_grid grid{};
+    std::vector<int8_t> sigma;
+    uint16_t *C = nullptr;    // BF16 [N][2][Na][Nj]
+    uint16_t *Phi = nullptr;  // BF16 [2][Fp][Nj]
+    uint16_t *W = nullptr;    // BF16 [2][bn][Nj]
+    int32_t *faces = nullptr;
+    double *lam = nullptr, *w = nullptr, *force = nullptr, *dwpart = nullptr;
+    float *u = nullptr;
+    float4 *parts = nullptr;
+    int32_t *perm = nullptr;
+    CUtensorMap mapC{}, mapPhi{}, mapW{};
+};
+
+}  // namespace
+
+struct psf_batch {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<HostGroup> groups;
+    std::vector<psf::SlotDev> slots;  // host mirror of the slot table
+    std::vector<psf::TraceItem> items;
+    psf::GroupDev *d_groups = nullptr;
+    psf::SlotDev *d_slots = nullptr;
+    psf::TraceItem *d_items = nullptr;
+    int *d_n_items = nullptr;
+    int *d_err = nullptr;
+    int64_t item_cap = 0;
+    psf::GemmArgs contract{};
+    psf::GemmArgs recon{};
+    int bn_max = 64;
+    int gemm_ctas = 148;
+    int trace_ctas = 592;
+    double tuned_ms = 0.0;
+    psf::OrderBufs order{};
+    int64_t pmax_all = 0;
+    int64_t bytes = 0;
+    std::vector<void *> allocs;
+
+    ~psf_batch()
+    {
+        drop_graph();
+        for (void *p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void drop_graph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    template <class T>
+    int alloc(T **p, size_t count)
+    {
+        void *v = nullptr;
+        const size_t n = std::max<size_t>(1, count) * sizeof(T);
+        cudaError_t e = cudaMalloc(&v, n);
+        if (e != cudaSuccess) return psf::cuda_fail(e, "cudaMalloc");
+        allocs.push_back(v);
+        bytes += (int64_t)n;
+        *p = static_cast<T *>(v);
+        return PSF_OK;
+    }
+    int n_slots() const { return (int)slots.size(); }
+};
+
+namespace {
+
+int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
+{
+    const psf_basis_desc &b = bb.basis;
+    const int N = G.N;
+    cudaStream_t st = B->stream;
+    // C as BF16 hi/lo [k][hl][a][j], a padded to Na and j to Nj with zeros.
+    {
+        std::vector<uint16_t> h((size_t)N * 2 * G.Na * G.Nj, 0);
+        for (int k = 0; k < N; ++k)
+            for (int a = 0; a < N; ++a) {
+                const double *src = b.advection + ((size_t)k * N + a) * N;
+                uint16_t *hi = h.data() + (((size_t)k * 2 + 0) * G.Na + a) * G.Nj;
+                uint16_t *lo = h.data() + (((size_t)k * 2 + 1) * G.Na + a) * G.Nj;
+                for (int j = 0; j < N; ++j) psf::split_bf16_host(src[j], hi + j, lo + j);
+            }
+        PSF_CHECK(B->alloc(&G.C, h.size()));
+        PSF_CUDA(cudaMemcpyAsync(G.C, h.data(), h.size() * 2, cudaMemcpyHostToDevice, st));
+        PSF_CUDA(cudaStreamSynchronize(st));
+    }
+    // Phi (tracer signs folded in) as BF16 hi/lo [hl][f][i], f padded to Fp.
+    {
+        std::vector<uint16_t> h((size_t)2 * G.Fp * G.Nj, 0);
+        for (int64_t r = 0; r < G.F_act; ++r) {
+            const double s = (double)G.sigma[(size_t)b.active_faces[r]];
+            uint16_t *hi = h.data() + ((size_t)0 * G.Fp + r) * G.Nj;
+            uint16_t *lo = h.data() + ((size_t)1 * G.Fp + r) * G.Nj;
+            for (int i = 0; i < N; ++i) psf::split_bf16_host(s * b.phi[(size_t)r * N + i], hi + i, lo + i);
+        }
+        PSF_CHECK(B->alloc(&G.Phi, h.size()));
+        PSF_CUDA(cudaMemcpyAsync(G.Phi, h.data(), h.size() * 2, cudaMemcpyHostToDevice, st));
+        PSF_CUDA(cudaStreamSynchronize(st));
+    }
+    PSF_CHECK(B->alloc(&G.faces, (size_t)G.F_act));
+    PSF_CHECK(B->alloc(&G.lam, (size_t)N));
+    PSF_CUDA(cudaMemcpyAsync(G.faces, b.active_faces, (size_t)G.F_act * 4, cudaMemcpyHostToDevice, st));
+    PSF_CUDA(cudaMemcpyAsync(G.lam, b.eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st));
+
+    const size_t cap = (size_t)G.cap;
+    PSF_CHECK(B->alloc(&G.W, (size_t)2 * G.bn * G.Nj));
+    PSF_CHECK(B->alloc(&G.w, cap * N));
+    PSF_CHECK(B->alloc(&G.force, cap * N));
+    PSF_CHECK(B->alloc(&G.dwpart, (size_t)N * G.a_tiles * 4 * cap));
+    PSF_CHECK(B->alloc(&G.u, cap * (size_t)G.n_faces));
+    PSF_CHECK(B->alloc(&G.parts, cap * (size_t)G.pmax));
+    PSF_CHECK(B->alloc(&G.perm, cap * (size_t)G.pmax));
+    PSF_CUDA(cudaMemsetAsync(G.W, 0, (size_t)2 * G.bn * G.Nj * 2, st));
+    PSF_CUDA(cudaMemsetAsync(G.w, 0, cap * N * 8, st));
+    PSF_CUDA(cudaMemsetAsync(G.force, 0, cap * N * 8, st));
+    PSF_CUDA(cudaMemsetAsync(G.dwpart, 0, (size_t)N * G.a_tiles * 4 * cap * 8, st));
+    PSF_CUDA(cudaMemsetAsync(G.u, 0, cap * (size_t)G.n_faces * 4, st));
+
+    // Tensor maps: inner dimension first, strides in bytes for dims 1..
+    {
+        const uint64_t dims[4] = {(uint64_t)G.Nj, (uint64_t)G.Na, 2, (uint64_t)N};
+        const uint64_t str[3] = {(uint64_t)G.Nj * 2, (uint64_t)G.Na * G.Nj * 2, (uint64_t)2 * G.Na * G.Nj * 2};
+        const uint32_t box[4] = {64, 128, 2, 1};
+        PSF_CHECK(psf::encode_tensor_map(&G.mapC, G.C, 4, dims, str, box));
+    }
+    {
+        const uint64_t dims[4] = {(uint64_t)G.Nj, (uint64_t)G.Fp, 2, 1};
+        const uint64_t str[3] = {(uint64_t)G.Nj * 2, (uint64_t)G.Fp * G.Nj * 2, (uint64_t)2 * G.Fp * G.Nj * 2};
+        const uint32_t box[4] = {64, 128, 2, 1};
+        PSF_CHECK(psf::encode_tensor_map(&G.mapPhi, G.Phi, 4, dims, str, box));
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)G.Nj, (uint64_t)G.bn, 2};
+        const uint64_t str[2] = {(uint64_t)G.Nj * 2, (uint64_t)G.bn * G.Nj * 2};
+        const uint32_t box[3] = {64, (uint32_t)G.bn, 2};
+        PSF_CHECK(psf::encode_tensor_map(&G.mapW, G.W, 3, dims, str, box));
+    }
+    return PSF_OK;
+}
+
+void fill_gemm_args(psf_batch *B)
+{
+    psf::GemmArgs &c = B->contract;
+    psf::GemmArgs &r = B->recon;
+    std::memset(&c, 0, sizeof(c));
+    std::memset(&r, 0, sizeof(r));
+    c.n_groups = r.n_groups = (int)B->groups.size();
+    c.err = r.err = B->d_err;
+    for (size_t gi = 0; gi < B->groups.size(); ++gi) {
+        HostGroup &G = B->groups[gi];
+        const uint32_t tx = 2u * 128u * 128u + 2u * (uint32_t)G.bn * 128u;
+        psf::GemmGroup &x = c.g[gi];
+        x.tmA = G.mapC;
+        x.tmB = G.mapW;
+        x.m_inner = G.a_tiles;
+        x.tiles = G.N * G.a_tiles;
+        x.k_chunks = G.Nj / 64;
+        x.bn = G.bn;
+        x.tx_bytes = tx;
+        x.cap = G.cap;
+        x.n_rows = G.N;
+        x.ldw = G.N;
+        x.w = G.w;
+        x.dwpart = G.dwpart;
+        c.total_tiles += x.tiles;
+        psf::GemmGroup &y = r.g[gi];
+        y.tmA = G.mapPhi;
+        y.tmB = G.mapW;
+        y.tiles = (int)(G.Fp / 128);
+        y.m_inner = y.tiles;
+        y.k_chunks = G.Nj / 64;
+        y.bn = G.bn;
+        y.tx_bytes = tx;
+        y.cap = G.cap;
+        y.n_rows = (int)G.F_act;
+        y.ldw = G.N;
+        y.faces = G.faces;
+        y.u = G.u;
+        y.n_faces = G.n_faces;
+        r.total_tiles += y.tiles;
+    }
+}
+
+int upload_tables(psf_batch *B)
+{
+    std::vector<psf::GroupDev> gd(B->groups.size());
+    for (size_t gi = 0; gi < B->groups.size(); ++gi) {
+        const HostGroup &G = B->groups[gi];
+        psf::GroupDev &d = gd[gi];
+        d.grid = psf::make_grid_dev(G.grid);
+        d.N = G.N;
+        d.Nj = G.Nj;
+        d.cap = G.cap;
+        d.bn = G.bn;
+        d.a_tiles = G.a_tiles;
+        d.slot_base = G.slot_base;
+        d.n_faces = G.n_faces;
+        d.pmax = G.pmax;
+        d.w = G.w;
+        d.force = G.force;
+        d.lam = G.lam;
+        d.dwpart = G.dwpart;
+        d.W = G.W;
+        d.u = G.u;
+        d.parts = G.parts;
+        d.perm = G.perm;
+    }
+    PSF_CUDA(cudaMemcpyAsync(B->d_groups, gd.data(), gd.size() * sizeof(psf::GroupDev), cudaMemcpyHostToDevice,
+                             B->stream));
+    PSF_CUDA(cudaMemcpyAsync(B->d_slots, B->slots.data(), B->slots.size() * sizeof(psf::SlotDev),
+                             cudaMemcpyHostToDevice, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return PSF_OK;
+}
+
+int upload_items(psf_batch *B)
+{
+    B->items.clear();
+    for (const HostGroup &G : B->groups)
+        for (int b = 0; b < G.cap; ++b) {
+            const psf::SlotDev &s = B->slots[(size_t)(G.slot_base + b)];
+            if (!s.active) continue;
+            for (int64_t st = 0; st < s.n_particles; st += 256)
+                B->items.push_back({G.slot_base + b, (int)st, (int)std::min<int64_t>(256, s.n_particles - st), 0});
+        }
+    const int n = (int)B->items.size();
+    if (n > 0)
+        PSF_CUDA(cudaMemcpyAsync(B->d_items, B->items.data(), (size_t)n * sizeof(psf::TraceItem),
+                                 cudaMemcpyHostToDevice, B->stream));
+    PSF_CUDA(cudaMemcpyAsync(B->d_n_items, &n, sizeof(int), cudaMemcpyHostToDevice, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return PSF_OK;
+}
+
+int check_device_error(psf_batch *B)
+{
+    int code = 0;
+    PSF_CUDA(cudaMemcpyAsync(&code, B->d_err, sizeof(int), cudaMemcpyDeviceToHost, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    if (code != 0) return fail(PSF_ERR_TIMEOUT, "a tensor-core kernel gave up a bounded wait (code " +
+                                                    std::to_string(code) + "); destroy the batch");
+    return PSF_OK;
+}
+
+// Project-written autotuner: time every kernel variant that fits the batch
+// (MMA columns 64 / 128 / 256, i.e. 4 / 3 / 2 pipeline stages, and persistent
+// grids of 1x and 1/2x the SM count) on both GEMMs and keep the fastest.
+int autotune(psf_batch *B, int need_bn)
+{
+    const int variants[3] = {64, 128, 256};
+    const int grids[2] = {B->num_sms, std::max(1, B->num_sms / 2)};
+    cudaEvent_t e0, e1;
+    PSF_CUDA(cudaEventCreate(&e0));
+    PSF_CUDA(cudaEventCreate(&e1));
+    double best = 1e30;
+    int best_bn = -1, best_grid = B->num_sms;
+    int rc = PSF_OK;
+    for (int v : variants) {
+        if (v < need_bn) continue;
+        for (int g : grids) {
+            for (int rep = 0; rc == PSF_OK && rep < 2; ++rep) {
+                rc = psf::launch_batch_gemm(B->contract, 0, v, g, B->stream);
+                if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, v, g, B->stream);
+            }
+            const int reps = 5;
+            cudaEventRecord(e0, B->stream);
+            for (int rep = 0; rc == PSF_OK && rep < reps; ++rep) {
+                rc = psf::launch_batch_gemm(B->contract, 0, v, g, B->stream);
+                if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, v, g, B->stream);
+            }
+            cudaEventRecord(e1, B->stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "autotune");
+            if (rc == PSF_OK) rc = check_device_error(B);
+            if (rc != PSF_OK) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms / reps < best) {
+                best = ms / reps;
+                best_bn = v;
+                best_grid = g;
+            }
+        }
+        if (rc != PSF_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != PSF_OK) return rc;
+    B->bn_max = best_bn;
+    B->gemm_ctas = best_grid;
+    B->tuned_ms = best;
+    return PSF_OK;
+}
+
+int launch_step(psf_batch *B, cudaStream_t st)
+{
+    PSF_CHECK(psf::launch_batch_gemm(B->contract, 0, B->bn_max, B->gemm_ctas, st));
+    PSF_CHECK(psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st));
+    PSF_CHECK(psf::launch_batch_gemm(B->recon, 1, B->bn_max, B->gemm_ctas, st));
+    PSF_CHECK(psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_items, B->d_n_items, B->trace_ctas, st));
+    return PSF_OK;
+}
+
+int build_graph(psf_batch *B)
+{
+    if (B->exec) return PSF_OK;
+    PSF_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_step(B, B->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+    if (rc != PSF_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return psf::cuda_fail(e, "cudaStreamEndCapture");
+    B->graph = g;
+    PSF_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+    return PSF_OK;
+}
+
+int slot_index(psf_batch *B, int32_t basis, int32_t slot, int *sg)
+{
+    if (!B) return fail(PSF_ERR_INVALID, "null batch");
+    if (basis < 0 || basis >= (int)B->groups.size()) return fail(PSF_ERR_INVALID, "basis index out of range");
+    if (slot < 0 || slot >= B->groups[(size_t)basis].cap) return fail(PSF_ERR_INVALID, "slot index out of range");
+    *sg = B->groups[(size_t)basis].slot_base + slot;
+    return PSF_OK;
+}
+
+psf::PlainDev particle_view(psf_batch *B, int basis, int slot, int64_t count)
+{
+    HostGroup &G = B->groups[(size_t)basis];
+    psf::PlainDev d{};
+    d.grid = psf::make_grid_dev(G.grid);
+    d.P = count;
+    d.parts = G.parts + (size_t)slot * G.pmax;
+    d.perm = G.perm + (size_t)slot * G.pmax;
+    return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
+{
+    if (!cfg || !out || !cfg->bases) return fail(PSF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->n_bases < 1 || cfg->n_bases > PSF_BATCH_MAX_BASES)
+        return fail(PSF_ERR_UNSUPPORTED, "n_bases must be in [1, PSF_BATCH_MAX_BASES]");
+    if (cfg->precision != PSF_PRECISION_BF16X2)
+        return fail(PSF_ERR_UNSUPPORTED, "batches run the BF16 hi/lo tensor-core path (PSF_PRECISION_BF16X2)");
+    if (cfg->gemm_columns != 0 && cfg->gemm_columns != 64 && cfg->gemm_columns != 128 && cfg->gemm_columns != 256)
+        return fail(PSF_ERR_INVALID, "gemm_columns must be 0, 64, 128 or 256");
+    int need_bn = 16;
+    for (int i = 0; i < cfg->n_bases; ++i) {
+        const psf_batch_basis &bb = cfg->bases[i];
+        const psf_basis_desc &b = bb.basis;
+        if (bb.slots < 1 || bb.slots > PSF_BATCH_MAX_SLOTS)
+            return fail(PSF_ERR_UNSUPPORTED, "slots per basis must be in [1, PSF_BATCH_MAX_SLOTS]");
+        if (bb.max_particles < 0 || bb.max_particles > INT32_MAX)
+            return fail(PSF_ERR_INVALID, "max_particles out of range");
+        if (b.n_modes < 1 || b.n_modes > psf::PSF_MAX_MODES)
+            return fail(PSF_ERR_UNSUPPORTED, "n_modes must be in [1, 1024]");
+        if (b.n_active < 1 || !b.active_faces || !b.phi || !b.advection || !b.eigenvalues || !b.sign_bits)
+            return fail(PSF_ERR_INVALID, "basis arrays must not be null");
+        if (b.grid.dims[0] == 0 || b.grid.dims[1] == 0 || b.grid.dims[2] == 0 || !(b.grid.resolution > 0.0))
+            return fail(PSF_ERR_INVALID, "grid dims and resolution must be positive");
+        const int64_t F = psf::n_faces_of(b.grid);
+        if (F >= (int64_t)INT32_MAX) return fail(PSF_ERR_UNSUPPORTED, "grid has too many faces");
+        for (int64_t r = 0; r < b.n_active; ++r)
+            if (b.active_faces[r] < 0 || b.active_faces[r] >= F)
+                return fail(PSF_ERR_INVALID, "active face id out of range");
+        need_bn = std::max(need_bn, (int)round_up(bb.slots, 16));
+    }
+    if (cfg->gemm_columns != 0 && cfg->gemm_columns < need_bn)
+        return fail(PSF_ERR_INVALID, "gemm_columns is smaller than the slots of a basis");
+
+    psf_batch *B = nullptr;
+    try {
+        B = new psf_batch();
+    } catch (const std::bad_alloc &) {
+        return fail(PSF_ERR_NOMEM, "host allocation failed");
+    }
+    auto bail = [&](int rc) {
+        delete B;
+        return rc;
+    };
+    B->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaSetDevice"));
+    cudaDeviceGetAttribute(&B->num_sms, cudaDevAttrMultiProcessorCount, device);
+    e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaStreamCreate"));
+    int rc = PSF_OK;
+    if ((rc = B->alloc(&B->d_err, 1)) != PSF_OK) return bail(rc);
+    if ((e = cudaMemsetAsync(B->d_err, 0, sizeof(int), B->stream)) != cudaSuccess)
+        return bail(psf::cuda_fail(e, "cudaMemset"));
+
+    int slot_base = 0;
+    B->groups.resize((size_t)cfg->n_bases);
+    try {
+        for (int i = 0; i < cfg->n_bases; ++i) {
+            const psf_batch_basis &bb = cfg->bases[i];
+            HostGroup &G = B->groups[(size_t)i];
+            G.N = bb.basis.n_modes;
+            G.Nj = (int)round_up(G.N, 64);
+            G.Na = (int)round_up(G.N, 128);
+            G.a_tiles = G.Na / 128;
+            G.cap = bb.slots;
+            G.bn = (int)round_up(bb.slots, 16);
+            G.slot_base = slot_base;
+            G.F_act = bb.basis.n_active;
+            G.Fp = round_up(G.F_act, 128);
+            G.grid = bb.basis.grid;
+            G.n_faces = psf::n_faces_of(G.grid);
+            G.pmax = round_up(std::max<int64_t>(1, bb.max_particles), 256);
+            B->pmax_all = std::max(B->pmax_all, G.pmax);
+            slot_base += G.cap;
+            if ((rc = psf::fold_signs(G.grid, bb.basis.sign_bits, G.sigma)) != PSF_OK) return bail(rc);
+            if ((rc = upload_basis(B, G, bb)) != PSF_OK) return bail(rc);
+        }
+        B->slots.assign((size_t)slot_base, psf::SlotDev{});
+        for (const HostGroup &G : B->groups)
+            for (int b = 0; b < G.cap; ++b) {
+                psf::SlotDev &s = B->slots[(size_t)(G.slot_base + b)];
+                s.group = (int)(&G - B->groups.data());
+                s.slot = b;
+            }
+    } catch (const std::bad_alloc &) {
+        return bail(fail(PSF_ERR_NOMEM, "host staging allocation failed"));
+    }
+    for (const HostGroup &G : B->groups) B->item_cap += (int64_t)G.cap * (G.pmax / 256);
+    if ((rc = B->alloc(&B->d_groups, B->groups.size())) || (rc = B->alloc(&B->d_slots, B->slots.size())) ||
+        (rc = B->alloc(&B->d_items, (size_t)B->item_cap)) || (rc = B->alloc(&B->d_n_items, 1)))
+        return bail(rc);
+    // Particle ordering scratch, sized for the largest slot.
+    {
+        psf::OrderBufs &o = B->order;
+        size_t tmp = 0;
+        unsigned char *temp = nullptr;
+        if ((rc = psf::sort_particles_temp_bytes(B->pmax_all, &tmp)) || (rc = B->alloc(&o.staging, B->pmax_all)) ||
+            (rc = B->alloc(&o.keys_in, B->pmax_all)) || (rc = B->alloc(&o.keys_out, B->pmax_all)) ||
+            (rc = B->alloc(&o.idx_in, B->pmax_all)) || (rc = B->alloc(&temp, tmp)))
+            return bail(rc);
+        o.temp = temp;
+        o.temp_bytes = tmp;
+    }
+    if ((rc = upload_tables(B)) != PSF_OK || (rc = upload_items(B)) != PSF_OK) return bail(rc);
+    fill_gemm_args(B);
+    B->trace_ctas = psf::batch_trace_grid(B->num_sms);
+    B->gemm_ctas = cfg->gemm_ctas > 0 ? cfg->gemm_ctas : B->num_sms;
+    if (cfg->gemm_columns != 0) {
+        B->bn_max = cfg->gemm_columns;
+    } else if (cfg->autotune) {
+        if ((rc = autotune(B, need_bn)) != PSF_OK) return bail(rc);
+        if (cfg->gemm_ctas > 0) B->gemm_ctas = cfg->gemm_ctas;
+    } else {
+        B->bn_max = need_bn <= 64 ? 64 : (need_bn <= 128 ? 128 : 256);
+    }
+    *out = B;
+    return PSF_OK;
+}
+
+int psf_batch_destroy(psf_batch *B)
+{
+    if (!B) return PSF_OK;
+    cudaSetDevice(B->device);
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    delete B;
+    return PSF_OK;
+}
+
+int psf_batch_info_get(psf_batch *B, psf_batch_info *info)
+{
+    if (!B || !info) return fail(PSF_ERR_INVALID, "null argument");
+    info->gemm_columns = B->bn_max;
+    info->gemm_ctas = B->gemm_ctas;
+    info->trace_ctas = B->trace_ctas;
+    info->kernels_per_step = 4;
+    info->device_bytes = B->bytes;
+    info->tuned_ms = B->tuned_ms;
+    return PSF_OK;
+}
+
+int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_instance_desc *inst)
+{
+    int sg = 0;
+    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    if (!inst || !inst->w0) return fail(PSF_ERR_INVALID, "null argument");
+    HostGroup &G = B->groups[(size_t)basis];
+    const psf_params &p = inst->params;
+    if (inst->n_modes < 1 || inst->n_modes > G.N)
+        return fail(PSF_ERR_INVALID, "n_modes must be in [1, the basis' n_modes]");
+    if (inst->n_particles < 0 || inst->n_particles > G.pmax)
+        return fail(PSF_ERR_INVALID, "n_particles exceeds the slot's capacity");
+    if (inst->n_particles > 0 && !inst->particles) return fail(PSF_ERR_INVALID, "particles is null");
+    if (!(p.timestep > 0.0) || !std::isfinite(p.timestep))
+        return fail(PSF_ERR_INVALID, "timestep must be positive and finite");
+    if (p.integrator != PSF_RK1 && p.integrator != PSF_RK4)
+        return fail(PSF_ERR_INVALID, "integrator must be PSF_RK1 or PSF_RK4");
+    if ((p.flags & PSF_FLAG_FORCING) && !inst->forcing)
+        return fail(PSF_ERR_INVALID, "PSF_FLAG_FORCING is set but forcing is null");
+    PSF_CUDA(cudaSetDevice(B->device));
+    cudaStream_t st = B->stream;
+    std::vector<double> row((size_t)G.N, 0.0), frow((size_t)G.N, 0.0);
+    std::memcpy(row.data(), inst->w0, (size_t)inst->n_modes * 8);
+    if (inst->forcing) std::memcpy(frow.data(), inst->forcing, (size_t)inst->n_modes * 8);
+    PSF_CUDA(cudaMemcpyAsync(G.w + (size_t)slot * G.N, row.data(), row.size() * 8, cudaMemcpyHostToDevice, st));
+    PSF_CUDA(cudaMemcpyAsync(G.force + (size_t)slot * G.N, frow.data(), frow.size() * 8, cudaMemcpyHostToDevice, st));
+    psf::SlotDev &s = B->slots[(size_t)sg];
+    s.active = 1;
+    s.n_modes = inst->n_modes;
+    s.rk4 = p.integrator == PSF_RK4;
+    s.flags = p.flags;
+    s.dt = p.timestep;
+    s.visc_signed = (p.flags & PSF_FLAG_DECAY_NEG) ? -p.viscosity : p.viscosity;
+    s.lifetime = p.lifetime;
+    s.seed = p.seed;
+    s.step = 0;
+    s.n_particles = inst->n_particles;
+    PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, st));
+    PSF_CHECK(psf::launch_batch_pack(B->d_groups, B->d_slots, sg, st));
+    if (inst->n_particles > 0) {
+        PSF_CUDA(cudaMemcpyAsync(B->order.staging, inst->particles, (size_t)inst->n_particles * 16,
+                                 cudaMemcpyHostToDevice, st));
+        PSF_CHECK(psf::launch_order_particles(particle_view(B, basis, slot, inst->n_particles), B->order, st));
+    }
+    PSF_CHECK(upload_items(B));
+    PSF_CUDA(cudaStreamSynchronize(st));
+    return PSF_OK;
+}
+
+int psf_batch_clear_instance(psf_batch *B, int32_t basis, int32_t slot)
+{
+    int sg = 0;
+    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    PSF_CUDA(cudaSetDevice(B->device));
+    HostGroup &G = B->groups[(size_t)basis];
+    psf::SlotDev &s = B->slots[(size_t)sg];
+    s.active = 0;
+    s.n_particles = 0;
+    PSF_CUDA(cudaMemsetAsync(G.w + (size_t)slot * G.N, 0, (size_t)G.N * 8, B->stream));
+    PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, B->stream));
+    PSF_CHECK(psf::launch_batch_pack(B->d_groups, B->d_slots, sg, B->stream));
+    PSF_CHECK(upload_items(B));
+    return PSF_OK;
+}
+
+int psf_batch_step(psf_batch *B, int32_t nsteps)
+{
+    if (!B) return fail(PSF_ERR_INVALID, "null batch");
+    if (nsteps < 0) return fail(PSF_ERR_INVALID, "nsteps must be >= 0");
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CHECK(build_graph(B));
+    for (int32_t i = 0; i < nsteps; ++i) PSF_CUDA(cudaGraphLaunch(B->exec, B->stream));
+    return PSF_OK;
+}
+
+int psf_batch_sync(psf_batch *B)
+{
+    if (!B) return fail(PSF_ERR_INVALID, "null batch");
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return check_device_error(B);
+}
+
+int psf_batch_get_stream(psf_batch *B, void **stream)
+{
+    if (!B || !stream) return fail(PSF_ERR_INVALID, "null argument");
+    *stream = (void *)B->stream;
+    return PSF_OK;
+}
+
+int psf_batch_get_state(psf_batch *B, int32_t basis, int32_t slot, double *w, int32_t n)
+{
+    int sg = 0;
+    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    if (!w) return fail(PSF_ERR_INVALID, "null argument");
+    const psf::SlotDev &s = B->slots[(size_t)sg];
+    if (!s.active) return fail(PSF_ERR_STATE, "slot is empty");
+    if (n != s.n_modes) return fail(PSF_ERR_INVALID, "n must equal the instance's n_modes");
+    HostGroup &G = B->groups[(size_t)basis];
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CUDA(cudaMemcpyAsync(w, G.w + (size_t)slot * G.N, (size_t)n * 8, cudaMemcpyDeviceToHost, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return check_device_error(B);
+}
+
+int psf_batch_get_particles(psf_batch *B, int32_t basis, int32_t slot, float *xyzw, int64_t count)
+{
+    int sg = 0;
+    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    const psf::SlotDev &s = B->slots[(size_t)sg];
+    if (count != s.n_particles) return fail(PSF_ERR_INVALID, "count must equal the instance's particle count");
+    if (count == 0) return PSF_OK;
+    if (!xyzw) return fail(PSF_ERR_INVALID, "null argument");
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CHECK(psf::launch_unorder_particles(particle_view(B, basis, slot, count), B->order, B->stream));
+    PSF_CUDA(cudaMemcpyAsync(xyzw, B->order.staging, (size_t)count * 16, cudaMemcpyDeviceToHost, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return check_device_error(B);
+}
+
+int psf_batch_get_velocity(psf_batch *B, int32_t basis, int32_t slot, float *u, int64_t n_faces)
+{
+    int sg = 0;
+    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    HostGroup &G = B->groups[(size_t)basis];
+    if (!u) return fail(PSF_ERR_INVALID, "null argument");
+    if (n_faces != G.n_faces) return fail(PSF_ERR_INVALID, "n_faces must equal the grid's face count");
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CUDA(cudaMemcpyAsync(u, G.u + (size_t)slot * G.n_faces, (size_t)n_faces * 4, cudaMemcpyDeviceToHost,
+                             B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    for (int64_t f = 0; f < n_faces; ++f) u[f] *= (float)G.sigma[(size_t)f];
+    return check_device_error(B);
+}
+
+int psf_batch_get_steps(psf_batch *B, int32_t basis, int32_t slot, int64_t *steps)
+{
+    int sg = 0;
+    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    if (!steps) return fail(PSF_ERR_INVALID, "null argument");
+    psf::SlotDev s{};
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CUDA(cudaMemcpyAsync(&s, B->d_slots + sg, sizeof(s), cudaMemcpyDeviceToHost, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    *steps = (int64_t)s.step;
+    return PSF_OK;
+}
+
+int psf_batch_profile_step(psf_batch *B, double *kernel_ms, int32_t n)
+{
+    if (!B || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
+    if (n < 4) return fail(PSF_ERR_INVALID, "kernel_ms needs 4 slots");
+    PSF_CUDA(cudaSetDevice(B->device));
+    cudaEvent_t ev[5];
+    for (int i = 0; i < 5; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
+    cudaStream_t st = B->stream;
+    int rc = PSF_OK;
+    cudaEventRecord(ev[0], st);
+    rc = psf::launch_batch_gemm(B->contract, 0, B->bn_max, B->gemm_ctas, st);
+    cudaEventRecord(ev[1], st);
+    if (rc == PSF_OK) rc = psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st);
+    cudaEventRecord(ev[2], st);
+    if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, B->bn_max, B->gemm_ctas, st);
+    cudaEventRecord(ev[3], st);
+    if (rc == PSF_OK)
+        rc = psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_items, B->d_n_items, B->trace_ctas, st);
+    cudaEventRecord(ev[4], st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");
+    for (int i = 0; rc == PSF_OK && i < 4; ++i) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        if (e != cudaSuccess) rc = psf::cuda_fail(e, "cudaEventElapsedTime");
+        kernel_ms[i] = ms;
+    }
+    for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+    if (rc == PSF_OK) rc = check_device_error(B);
+    return rc;
+}
+
+int psf_batch_device_status(psf_batch *B, int32_t *code)
+{
+    if (!B || !code) return fail(PSF_ERR_INVALID, "null argument");
+    int c = 0;
+    PSF_CUDA(cudaSetDevice(B->device));
+    PSF_CUDA(cudaMemcpyAsync(&c, B->d_err, sizeof(int), cudaMemcpyDeviceToHost, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    *code = c;
+    return PSF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+// Internal types of the batched engine (include/psf_batch.h), shared by the
+// kernels (psf_batch.cu) and the C ABI implementation (psf_batch_api.cpp).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "psf_internal.h"
+
+namespace psf {
+
+constexpr int BATCH_MAX_GROUPS = 6;   // distinct bases in one batch
+constexpr int BATCH_MAX_SLOTS = 256;  // instance slots per basis (one MMA N tile)
+constexpr int GEMM_THREADS = 192;     // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+
+// One basis inside a GEMM launch: A operand (C or Phi) and B operand (the
+// slots' coefficient vectors), both BF16 hi/lo pairs, K-major, 128-byte
+// swizzled by TMA.
+struct alignas(64) GemmGroup {
+    CUtensorMap tmA;        // 4D (k inner 64, rows 128, hi/lo 2, outer 1)
+    CUtensorMap tmB;        // 3D (k inner 64, bn rows, hi/lo 2)
+    int tiles;              // 128-row tiles of this basis
+    int m_inner;            // row tiles per outer index (contraction: a-tiles per mode k)
+    int k_chunks;           // K / 64
+    int bn;                 // MMA N: slots rounded up to 16
+    uint32_t tx_bytes;      // bytes one pipeline stage receives
+    int cap;                // slots in use (columns)
+    int n_rows;             // valid rows: N (contraction) or F_act (reconstruction)
+    int ldw;                // row stride of w (= the basis' N)
+    const double *w;        // contraction: FP64 state [cap][ldw]
+    double *dwpart;         // contraction: partials [((k*m_inner + at)*4 + q)][cap]
+    const int32_t *faces;   // reconstruction: reference face id of each row
+    float *u;               // reconstruction: face field [cap][n_faces]
+    long long n_faces;
+};
+
+struct GemmArgs {
+    GemmGroup g[BATCH_MAX_GROUPS];
+    int n_groups;
+    int total_tiles;
+    int *err;  // device error word (bounded waits)
+};
+
+// Per-slot parameters and counters, in device memory.
+struct SlotDev {
+    int active;
+    int n_modes;
+    int rk4;
+    int group;
+    int slot;
+    unsigned int flags;
+    double dt;
+    double visc_signed;
+    float lifetime;
+    float pad0;
+    unsigned long long seed;
+    unsigned long long step;  // steps taken since the slot was set (device counter)
+    long long n_particles;
+};
+
+// Per-basis device view used by the state kernel and the tracer.
+struct GroupDev {
+    GridDev grid;
+    int N, Nj, cap, bn, a_tiles, slot_base;
+    long long n_faces, pmax;
+    double *w;            // [cap][N]
+    double *force;        // [cap][N]
+    const double *lam;    // [N]
+    double *dwpart;       // see GemmGroup
+    uint16_t *W;          // BF16 [2][bn][Nj]
+    float *u;             // [cap][n_faces]
+    float4 *parts;        // [cap][pmax]
+    int32_t *perm;        // [cap][pmax]
+};
+
+// One tracer work item: up to 256 particles of one slot.
+struct TraceItem {
+    int slot_global;
+    int start;
+    int count;
+    int pad;
+};
+
+// Launchers (psf_batch.cu).  `bn_max` selects the kernel variant (64, 128 or
+// 256 MMA columns per accumulator); `grid` the number of persistent CTAs.
+int batch_gemm_smem_bytes(int bn_max);
+int launch_batch_gemm(const GemmArgs &args, int epilogue, int bn_max, int grid, cudaStream_t st);
+int launch_batch_state(const GroupDev *groups, SlotDev *slots, int n_slots, cudaStream_t st);
+int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const TraceItem *items, const int *n_items,
+                       int grid, cudaStream_t st);
+int launch_batch_pack(const GroupDev *groups, const SlotDev *slots, int slot_global, cudaStream_t st);
+int batch_trace_grid(int num_sms);
+
+// Host helpers.
+int encode_tensor_map(CUtensorMap *map, void *base, int rank, const uint64_t *dims, const uint64_t *strides_bytes,
+                      const uint32_t *box);
+void split_bf16_host(double x, uint16_t *hi, uint16_t *lo);
+
+}  // namespace psf

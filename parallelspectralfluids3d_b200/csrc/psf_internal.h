@@ -5,6 +5,9 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
+
+#include "psf_b200.h"
 
 namespace psf {
 
@@ -63,6 +66,15 @@ struct OrderBufs {
     void *temp = nullptr;
     size_t temp_bytes = 0;
 };
+
+// Number of faces of a grid in the reference numbering (z-, y-, then x-faces).
+int64_t n_faces_of(const psf_grid &g);
+// Sign (+1/-1) with which the reference tracer reads each face (0 for faces
+// no voxel reads); PSF_ERR_SIGNS if two voxels read a face with different signs.
+int fold_signs(const psf_grid &g, const uint32_t *bits, std::vector<int8_t> &sigma);
+
+// Tracer constants of a grid (the reference's index offsets and box).
+GridDev make_grid_dev(const psf_grid &g);
 
 extern thread_local std::string g_last_error;
 int fail(int code, const std::string &msg);

@@ -1,0 +1,164 @@
+"""Batched BF16 hi/lo tensor-core path (include/psf_batch.h) against the FP64 oracle.
+
+Every slot is checked against an FP64 rollout of the reference step on its
+own prefix basis.  Tolerances for the compensated BF16 products (each operand
+carries 16 significant bits, products accumulate in FP32): relative L2 error
+of w <= 1e-4 (the bar stated for this form), particles within 2e-3 voxel,
+face velocities within 1e-4 of max |u|.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from parallelspectralfluids3d_b200 import _lib as L
+from parallelspectralfluids3d_b200.batch import Batch
+from parallelspectralfluids3d_b200.fixture import initial_coefficients, initial_particles
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+W_TOL = 1e-4
+P_TOL_VOX = 2e-3
+U_TOL = 1e-4
+
+# (slot, n_modes, dt, flags, viscosity, integrator, particles, seed)
+SPECS = [
+    (0, 37, 0.02, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 300, 1),
+    (1, 20, 0.03, L.PSF_FLAG_RENORM | L.PSF_FLAG_FORCING, 0.0, L.PSF_RK1, 500, 2),
+    (2, 11, 0.05, L.PSF_FLAG_RENORM | L.PSF_FLAG_DECAY_NEG, 0.05, L.PSF_RK4, 257, 3),
+    (4, 37, 0.01, 0, 0.0, L.PSF_RK4, 700, 4),
+    (5, 30, 0.02, L.PSF_FLAG_RENORM, 0.02, L.PSF_RK1, 0, 5),
+]
+
+
+def _instance(b, spec):
+    slot, n, dt, flags, visc, integ, P, seed = spec
+    w0 = initial_coefficients(n, seed)
+    parts = initial_particles(b, P, seed + 50) if P else None
+    f = None
+    if flags & L.PSF_FLAG_FORCING:
+        f = np.zeros(n)
+        f[0] = 0.1 / dt
+    params = L.make_params(dt=dt, viscosity=visc, integrator=integ, flags=flags, seed=seed)
+    return w0, parts, f, params
+
+
+def _oracle(b, spec, steps):
+    slot, n, dt, flags, visc, integ, P, seed = spec
+    w0, parts, f, _ = _instance(b, spec)
+    oflags = (O.FLAG_RENORM if flags & L.PSF_FLAG_RENORM else 0) | (
+        O.FLAG_DECAY_NEG if flags & L.PSF_FLAG_DECAY_NEG else 0)
+    return O.OracleRollout(b.truncate(n), w0, parts, dt=dt, viscosity=visc, flags=oflags, integrator=integ,
+                           seed=seed, forcing=f).step(steps)
+
+
+def _fill(batch, b, specs, basis=0):
+    for spec in specs:
+        w0, parts, f, params = _instance(b, spec)
+        batch.set_instance(basis, spec[0], w0, params, particles=parts, forcing=f)
+
+
+def test_batch_slots_match_oracle(small_bases):
+    b = small_bases["sphere12x10x9"]
+    steps = 20
+    with Batch([b], slots=6, max_particles=1024) as batch:
+        _fill(batch, b, SPECS)
+        batch.step(steps)
+        batch.sync()
+        assert batch.device_status() == 0
+        for spec in SPECS:
+            ref = _oracle(b, spec, steps)
+            w = batch.get_state(0, spec[0])
+            assert rel_err(w, ref.w) <= W_TOL, (spec, rel_err(w, ref.w))
+            if spec[6]:
+                p = batch.get_particles(0, spec[0])
+                err = np.abs(p[:, :3] - ref.pos).max() / b.h
+                assert err <= P_TOL_VOX, (spec, err)
+                assert np.array_equal(p[:, 3], ref.life)
+            assert batch.get_steps(0, spec[0]) == steps
+
+
+def test_batch_one_step_velocity_field(small_bases):
+    b = small_bases["sphere12x10x9"]
+    spec = SPECS[0]
+    with Batch([b], slots=3, max_particles=512) as batch:
+        _fill(batch, b, [spec])
+        batch.step(1)
+        u = batch.get_velocity(0, spec[0])
+    ref = _oracle(b, spec, 1)
+    assert np.abs(u - ref.u).max() <= U_TOL * np.abs(ref.u).max()
+    mask = np.ones(b.n_faces, bool)
+    mask[b.active_faces] = False
+    assert np.all(u[mask] == 0)
+
+
+def test_alone_equals_in_the_mix(small_bases):
+    """A rollout gives the same result alone in a batch and among other rollouts."""
+    b = small_bases["sphere12x10x9"]
+    target = SPECS[0]
+    results = []
+    for others in ([], [s for s in SPECS if s[0] != target[0]]):
+        with Batch([b], slots=6, max_particles=1024) as batch:
+            _fill(batch, b, [target] + others)
+            batch.step(15)
+            results.append((batch.get_state(0, target[0]), batch.get_particles(0, target[0])))
+    (w_a, p_a), (w_m, p_m) = results
+    assert np.array_equal(w_a, w_m)
+    assert np.array_equal(p_a, p_m)
+
+
+@pytest.mark.parametrize("cols", [64, 128, 256])
+def test_kernel_variants_agree(small_bases, cols):
+    b = small_bases["sphere12x10x9"]
+    outs = []
+    for c in (0, cols):
+        with Batch([b], slots=6, max_particles=1024, autotune=False, gemm_columns=c) as batch:
+            _fill(batch, b, SPECS[:3])
+            batch.step(10)
+            outs.append(np.concatenate([batch.get_state(0, s[0]) for s in SPECS[:3]]))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_two_bases_in_one_batch(small_bases):
+    b1, b2 = small_bases["sphere12x10x9"], small_bases["box576"]
+    s1 = (1, 25, 0.02, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 400, 7)
+    s2 = (0, 13, 0.04, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 333, 8)
+    with Batch([b1, b2], slots=[2, 3], max_particles=[512, 512]) as batch:
+        _fill(batch, b1, [s1], basis=0)
+        _fill(batch, b2, [s2], basis=1)
+        batch.step(12)
+        for bb, spec, gi in ((b1, s1, 0), (b2, s2, 1)):
+            ref = _oracle(bb, spec, 12)
+            assert rel_err(batch.get_state(gi, spec[0]), ref.w) <= W_TOL
+            p = batch.get_particles(gi, spec[0])
+            assert np.abs(p[:, :3] - ref.pos).max() / bb.h <= P_TOL_VOX
+
+
+def test_clear_and_reuse_slot(small_bases):
+    b = small_bases["sphere12x10x9"]
+    with Batch([b], slots=2, max_particles=1024) as batch:
+        _fill(batch, b, [SPECS[0]])
+        batch.step(5)
+        batch.clear_instance(0, 0)
+        batch.step(3)  # empty batch steps are no-ops for the cleared slot
+        spec = (0,) + SPECS[3][1:]
+        _fill(batch, b, [spec])
+        batch.step(10)
+        ref = _oracle(b, spec, 10)
+        assert rel_err(batch.get_state(0, 0), ref.w) <= W_TOL
+        assert batch.get_steps(0, 0) == 10
+
+
+def test_batch_argument_errors(small_bases):
+    b = small_bases["box6"]
+    with Batch([b], slots=2, max_particles=100) as batch:
+        w0 = initial_coefficients(b.n_modes, 0)
+        with pytest.raises(L.PSFError):
+            batch.set_instance(0, 2, w0, L.make_params())  # slot out of range
+        with pytest.raises(L.PSFError):
+            batch.set_instance(0, 0, np.zeros(b.n_modes + 1), L.make_params())  # too many modes
+        with pytest.raises(L.PSFError):
+            batch.set_instance(0, 0, w0, L.make_params(), particles=np.zeros((300, 4), np.float32))
+        with pytest.raises(L.PSFError):
+            batch.get_state(0, 1)  # empty slot
