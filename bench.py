@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from parallelspectralfluids3d_b200 import replicas  # noqa: E402
+
 WORKLOADS = {
     "sphere32_n128_p262144_rk4": dict(
         domain=("sphere", 32, 8.0), n_modes=128, seed_w=2, seed_p=3, particles=262144, dt=0.005,
@@ -45,7 +47,33 @@ WORKLOADS = {
         force0=0.0, integrator=4, full_steps=100,
         describe="16^3 all-wall box, N=64, 4096 particles, RK4, dt=0.01"),
 }
+# Batched (tensor-core, BF16 hi/lo) workloads.  "members" lists
+# (domain, n_max, slots, n_modes per instance, particles per instance).
+BATCH_WORKLOADS = {
+    # The plain workload above, 64 independent instances (seeds 2+i / 3+i) on one basis.
+    "sphere32_n128_p262144_rk4_b64": dict(
+        bases=[(("sphere", 32, 8.0), 128)], instances=64, n_modes=lambda i, rng: 128, particles=262144,
+        dt=0.005, force0=0.1, integrator=4, seed_w=lambda i: 2 + i, seed_p=lambda i: 3 + i, full_steps=1000,
+        check=[0, 63], check_particles=[0],
+        describe="64 instances of the 32^3 + sphere r=8, N=128, 262144-particle RK4 workload, one batch"),
+    # Precision form: 48^3 channel (all-wall box), N=256, B=64 trajectories, seeds 100-163, 1M particles each.
+    "channel48_n256_b64_p1m": dict(
+        bases=[(("channel", (48, 48, 48), None), 256)], instances=64, n_modes=lambda i, rng: 256,
+        particles=1 << 20, dt=0.005, force0=0.0, integrator=4, seed_w=lambda i: 100 + i,
+        seed_p=lambda i: 10100 + i, full_steps=1000, check=[0, 31, 63], check_particles=[],
+        describe="48^3 channel, N=256 (C, Phi as BF16 hi+lo), 64 trajectories x 1M particles, RK4, dt=0.005"),
+    # Batching form: 512 instances, N ~ U{32..256}, domains in rotation, 16384 particles each.
+    "mixed512_p16384": dict(
+        bases=[(("box", 32, None), 256), (("sphere", 40, 10.0), 256), (("channel", (64, 32, 32), None), 256)],
+        instances=512, n_modes=lambda i, rng: int(rng.choice([32, 64, 96, 128, 192, 256])), particles=16384,
+        dt=0.005, force0=0.0, integrator=4, seed_w=lambda i: 1000 + i, seed_p=lambda i: 5000 + i,
+        full_steps=500, check=[0, 1, 2, 511], check_particles=[0],
+        describe="512 instances, N uniform in {32,64,96,128,192,256}, domains 32^3 box / 40^3 + sphere r=10 / "
+                 "64x32x32 channel in rotation, 16384 particles each, RK4"),
+}
+BIG_BASIS_CACHE = os.path.join(ROOT, ".basis_big")
 DEFAULT_WORKLOAD = "sphere32_n128_p262144_rk4"
+FORM_WORKLOAD = "sphere32_n128_p262144_rk4_b64"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 # DRAM bytes (read + write) per launch from one ncu capture of each kernel on
@@ -58,10 +86,14 @@ NCU_TRAFFIC = {
 
 
 def make_domain(spec):
-    from parallelspectralfluids3d_b200.domain import box_domain, sphere_obstacle_domain
+    from parallelspectralfluids3d_b200.domain import box_domain, channel_domain, sphere_obstacle_domain
 
     kind, n, r = spec
-    return sphere_obstacle_domain(n, r) if kind == "sphere" else box_domain(n)
+    if kind == "sphere":
+        return sphere_obstacle_domain(n, r)
+    if kind == "channel":
+        return channel_domain(n)
+    return box_domain(n)
 
 
 def load_workload(name, device):
@@ -214,10 +246,7 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     per_step = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
     total_ms = float(per_step.sum())
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        total_ms = float(t.item())
+    (total_ms,) = replicas.slowest([total_ms], device=dev)
     value = world * K / (total_ms / 1e3)
 
     # Kernel breakdown: each kernel between its own events, L2 flushed before each step.
@@ -260,10 +289,7 @@ def run_ours(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    (e2e_ms,) = replicas.slowest([e2e_ms], device=dev)
     e2e = {"value": round(world * E / (e2e_ms / 1e3), 2), "unit": "instance-steps/s",
            "h2d_bytes_per_step": int(8 * b.n_modes + 16 * ctx.P),
            "d2h_bytes_per_step": int(8 * b.n_modes + 16 * ctx.P), "steps": E}
@@ -292,6 +318,12 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "e2e": e2e, "clocks": clk,
     }
     line.update(extra)
+    if rank == 0 and world == 1 and not args.no_forms:
+        form = run_batch(args, FORM_WORKLOAD, local_rank)
+        form["speedup_vs_plain"] = round(form["value"] / value, 3)
+        form["e2e_speedup_vs_plain"] = round(form["e2e"]["value"] / e2e["value"], 3)
+        line["forms"] = {"batched_bf16x2": dict(workload=FORM_WORKLOAD, **form)}
+        line["gpu_launches"] += form["gpu_launches"]
     return line
 
 
@@ -327,6 +359,8 @@ def run_reference(args):
     """The reference's CPU step (FP64 restatement) on all host threads."""
     from oracle import oracle as O
 
+    if args.workload in BATCH_WORKLOADS:
+        return run_reference_batch(args)
     wl, b, w0, parts, force = load_workload(args.workload, "cpu")
     O.build()
     ref = O.OracleRollout(b, w0, parts, dt=wl["dt"], integrator=wl["integrator"], forcing=force)
@@ -349,6 +383,255 @@ def run_reference(args):
     }
 
 
+# ------------------------------------------------------------ batched arm
+def load_batch_workload(name, device):
+    """Bases and per-instance inputs of a batched workload (seeded, synthetic)."""
+    from parallelspectralfluids3d_b200.fixture import cached_basis, initial_coefficients, initial_particles
+
+    wl = BATCH_WORKLOADS[name]
+    bases = []
+    for spec, n in wl["bases"]:
+        dom = make_domain(spec)
+        small = os.path.join(ROOT, ".basis_cache")
+        cache = small if os.path.exists(os.path.join(small, f"{dom.name}_n{n}.psfb")) else BIG_BASIS_CACHE
+        bases.append(cached_basis(dom, n, cache_dir=cache, device=device))
+    rng = np.random.default_rng(4)
+    insts = []
+    for i in range(wl["instances"]):
+        g = i % len(bases)
+        n = wl["n_modes"](i, rng)
+        w0 = initial_coefficients(n, wl["seed_w"](i))
+        f = np.zeros(n)
+        f[0] = wl["force0"] / wl["dt"]
+        insts.append(dict(basis=g, slot=i // len(bases), n=n, w0=w0, force=f, seed_p=wl["seed_p"](i)))
+    slots = [sum(1 for x in insts if x["basis"] == g) for g in range(len(bases))]
+    for x in insts:
+        x["parts"] = initial_particles(bases[x["basis"]], wl["particles"], x["seed_p"])
+    return wl, bases, slots, insts
+
+
+def batch_params(wl, x):
+    from parallelspectralfluids3d_b200 import _lib as L
+
+    flags = L.PSF_FLAG_RENORM | (L.PSF_FLAG_FORCING if wl["force0"] else 0)
+    return L.make_params(dt=wl["dt"], integrator=wl["integrator"], flags=flags, seed=x["seed_p"],
+                         precision=L.PSF_PRECISION_BF16X2)
+
+
+def fill_batch(batch, wl, insts):
+    for x in insts:
+        batch.set_instance(x["basis"], x["slot"], x["w0"], batch_params(wl, x), particles=x["parts"],
+                           forcing=x["force"] if wl["force0"] else None)
+
+
+def batch_kernel_bytes(bases, slots, insts, kind):
+    """Algorithmic bytes (and tensor FLOPs) of one launch of a batched kernel."""
+    tot, flops = 0, 0
+    for b, cap in zip(bases, slots):
+        N, Fa = b.n_modes, b.n_active
+        at = (N + 127) // 128
+        if kind == "contract":
+            tot += 4 * N ** 3 + 8 * N * cap + 32 * N * at * cap
+            flops += 3 * 2 * N * N * ((N + 63) // 64 * 64) * ((cap + 15) // 16 * 16)
+        elif kind == "reconstruct":
+            tot += 4 * Fa * N + 8 * Fa * cap
+            flops += 3 * 2 * Fa * ((N + 63) // 64 * 64) * ((cap + 15) // 16 * 16)
+        elif kind == "state":
+            tot += cap * (8 * N * 2 + 8 * N * at * 4 + 4 * N)
+    if kind == "trace":
+        tot = 32 * sum(len(x["parts"]) for x in insts)
+    return tot, flops
+
+
+def run_batch(args, name, local_rank, flush=True, check=True):
+    """Time a batched workload: device instance-steps/s, kernel roofline, e2e rollouts, FP64 error."""
+    import torch
+
+    from parallelspectralfluids3d_b200.batch import Batch
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    wl, bases, slots, insts = load_batch_workload(name, "cuda")
+    P = wl["particles"]
+    t0 = time.perf_counter()
+    batch = Batch(bases, slots=slots, max_particles=P, device=local_rank, autotune=True)
+    tune_s = time.perf_counter() - t0
+    fill_batch(batch, wl, insts)
+    stream = torch.cuda.ExternalStream(batch.stream, device=dev)
+    flush_w = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sink = torch.empty((), dtype=torch.float32, device=dev)
+    K = max(1, args.batch_steps)
+    batch.step(max(3, args.warmup))
+    batch.sync()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for i in range(K):
+            if flush:
+                flush_w.zero_()
+                torch.sum(flush_r, dim=0, out=sink)
+            starts[i].record(stream)
+            batch.step(1)
+            ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    per_step = np.array([a.elapsed_time(b) for a, b in zip(starts, ends)])
+    total_ms = float(per_step.sum())
+    B = len(insts)
+    value = B * K / (total_ms / 1e3)
+    # Per kernel, L2 flushed before each profiled step.
+    names = ["contract", "state", "reconstruct", "trace"]
+    acc = np.zeros(4)
+    M = min(K, 20)
+    for _ in range(M):
+        with torch.cuda.stream(stream):
+            flush_w.zero_()
+            torch.sum(flush_r, dim=0, out=sink)
+        acc += batch.profile_step()
+    kms = acc / M
+    peak, peak_kind = measured_peak_hbm()
+    tpeak = measured_peak_tensor()
+    kern = {}
+    for n_, m in zip(names, kms):
+        by, fl = batch_kernel_bytes(bases, slots, insts, n_)
+        kern[n_] = {"ms": round(float(m), 5), "algorithmic_bytes": int(by), "GB/s": round(by / (m / 1e3) / 1e9, 1),
+                    "frac_hbm": round(by / (m / 1e3) / 1e9 / peak, 4)}
+        if fl:
+            kern[n_]["TFLOP/s"] = round(fl / (m / 1e3) / 1e12, 1)
+            kern[n_]["frac_tensor"] = round(fl / (m / 1e3) / 1e12 / tpeak, 4)
+    dom = names[int(np.argmax(kms))]
+    roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["GB/s"], "peak": peak, "unit": "GB/s",
+            "frac": kern[dom]["frac_hbm"], "peak_source": peak_kind,
+            "algorithmic_bytes": kern[dom]["algorithmic_bytes"],
+            "traffic": NCU_TRAFFIC.get((name, dom)), "all_kernels": kern}
+    # End to end through the public API: every rollout set from host buffers,
+    # stepped, and read back (state and particles), per E steps.
+    E = max(1, min(K, 20))
+    t0e = torch.cuda.Event(enable_timing=True)
+    t1e = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    t0e.record(stream)
+    fill_batch(batch, wl, insts)
+    batch.step(E)
+    h2d = d2h = 0
+    for x in insts:
+        w = batch.get_state(x["basis"], x["slot"])
+        p = batch.get_particles(x["basis"], x["slot"])
+        d2h += w.nbytes + p.nbytes
+        h2d += x["w0"].nbytes + x["parts"].nbytes
+    t1e.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = t0e.elapsed_time(t1e)
+    e2e = {"value": round(B * E / (e2e_ms / 1e3), 2), "unit": "instance-steps/s",
+           "h2d_bytes_per_step": int(h2d // E), "d2h_bytes_per_step": int(d2h // E),
+           "rollout_steps": E}
+    out = {"value": round(value, 2), "unit": "instance-steps/s", "instances": B, "steps": K,
+           "ms_per_step": round(total_ms / K, 5), "p50_ms": round(float(np.percentile(per_step, 50)), 5),
+           "p99_ms": round(float(np.percentile(per_step, 99)), 5),
+           "particle_steps_per_s": round(value * P, 1), "kernel_ms": {n_: round(float(m), 5) for n_, m in zip(names, kms)},
+           "roofline": roof, "e2e": e2e, "gpu_launches": int(4 * K), "batch": batch.info(),
+           "autotune_s": round(tune_s, 3), "describe": wl["describe"]}
+    if check:
+        out["accuracy"] = batch_accuracy(batch, wl, bases, insts, local_rank)
+    batch.close()
+    return out
+
+
+def batch_accuracy(batch, wl, bases, insts, device):
+    """Relative error of w (and particle error) against the FP64 oracle after the full step count."""
+    from oracle import oracle as O
+
+    S = wl["full_steps"]
+    fill_batch(batch, wl, insts)
+    batch.step(S)
+    res = []
+    for i in wl["check"]:
+        x = insts[i]
+        b = bases[x["basis"]].truncate(x["n"])
+        withp = i in wl["check_particles"]
+        ref = O.OracleRollout(b, x["w0"], x["parts"] if withp else None, dt=wl["dt"], integrator=wl["integrator"],
+                              forcing=x["force"] if wl["force0"] else None, seed=x["seed_p"],
+                              reconstruct=withp).step(S)
+        w = batch.get_state(x["basis"], x["slot"])
+        r = {"instance": i, "n_modes": x["n"], "rel_err_w_vs_fp64": float(np.linalg.norm(w - ref.w) / np.linalg.norm(ref.w))}
+        if withp:
+            p = batch.get_particles(x["basis"], x["slot"])
+            d = np.abs(p[:, :3] - ref.pos).max(axis=1) / bases[x["basis"]].h
+            r["max_particle_err_voxels"] = float(d.max())
+            r["p99_particle_err_voxels"] = float(np.percentile(d, 99))
+        res.append(r)
+    return {"steps": S, "instances": res,
+            "max_rel_err_w": max(r["rel_err_w_vs_fp64"] for r in res)}
+
+
+def run_batch_line(args, rank, world, local_rank):
+    """Bench line of a batched workload (every rank runs its own batch: weak scaling)."""
+    import torch
+
+    args.batch_steps = args.steps if args.steps else args.batch_steps
+    clocks = ClockSampler(local_rank).start()
+    r = run_batch(args, args.workload, local_rank, check=(rank == 0 and world == 1 and not args.no_cpu))
+    clk = clocks.stop()
+    total_ms = r["ms_per_step"] * r["steps"]
+    e2e_v = r["e2e"]["value"]
+    total_ms, inv = replicas.slowest([total_ms, 1.0 / max(e2e_v, 1e-30)], device=torch.device("cuda", local_rank))
+    e2e_v = 1.0 / inv
+    value = world * r["instances"] * r["steps"] / (total_ms / 1e3)
+    e2e = dict(r["e2e"], value=round(world * e2e_v, 2))
+    line = {"metric": "instance-steps/s", "value": round(value, 2), "unit": "instance-steps/s", "n_gpus": world,
+            "steps": r["steps"], "warmup": max(3, args.warmup), "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x2",
+            "state_dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "describe": r["describe"], "instances_per_gpu": r["instances"],
+                       "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
+                       "parallelism": f"replicas x{world}"},
+            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "particle_steps_per_s": round(world * r["particle_steps_per_s"], 1),
+            "gpu_launches": r["gpu_launches"], "kernel_ms": r["kernel_ms"], "roofline": r["roofline"], "e2e": e2e,
+            "clocks": clk, "batch": r["batch"]}
+    if "accuracy" in r:
+        line["accuracy"] = r["accuracy"]
+    return line
+
+
+def measured_peak_tensor():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["bf16_tflops"])
+    return 1590.0
+
+
+
+def run_reference_batch(args):
+    """The reference CPU step on a bounded sample of a batched workload's instances."""
+    from oracle import oracle as O
+
+    O.build()
+    wl, bases, slots, insts = load_batch_workload(args.workload, "cpu")
+    K = max(1, min(args.steps, 10))
+    sample = insts[: min(len(insts), len(bases) * 2)]
+    rolls = [O.OracleRollout(bases[x["basis"]].truncate(x["n"]), x["w0"], x["parts"], dt=wl["dt"],
+                             integrator=wl["integrator"], forcing=x["force"] if wl["force0"] else None,
+                             seed=x["seed_p"]) for x in sample]
+    for r in rolls:
+        r.step(max(1, min(3, args.warmup)))
+    t0 = time.perf_counter()
+    for r in rolls:
+        r.step(K)
+    dt = time.perf_counter() - t0
+    value = len(rolls) * K / dt
+    desc = f"{K} steps of each of {len(rolls)} instances (one at a time, all threads), FP64"
+    return {
+        "impl": "reference", "metric": "instance-steps/s", "value": round(value, 3), "unit": "instance-steps/s",
+        "n_gpus": 1, "steps": K, "warmup": max(3, args.warmup), "ms_per_step": round(1e3 * dt / (K * len(rolls)), 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "describe": wl["describe"]},
+        "cpu_baseline": {"value": round(value, 3), "unit": "instance-steps/s", "cores": O.num_threads(),
+                         "kind": "port", "sample": desc},
+        "e2e": {"value": round(value, 3), "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def run_for_profiler(args):
     """Set up the workload and launch ``args.ncu`` steps kernel by kernel (for ncu captures)."""
     import torch
@@ -356,6 +639,22 @@ def run_for_profiler(args):
     from parallelspectralfluids3d_b200 import _lib as L
     from parallelspectralfluids3d_b200.solver import Context
 
+    if args.workload in BATCH_WORKLOADS:
+        from parallelspectralfluids3d_b200.batch import Batch
+
+        wl, bases, slots, insts = load_batch_workload(args.workload, "cuda")
+        if args.ncu_instances:
+            insts = insts[: args.ncu_instances]
+            slots = [max(1, sum(1 for x in insts if x["basis"] == g)) for g in range(len(bases))]
+        batch = Batch(bases, slots=slots, max_particles=wl["particles"], autotune=False)
+        fill_batch(batch, wl, insts)
+        for _ in range(args.ncu):
+            ms = batch.profile_step()
+        torch.cuda.synchronize()
+        print(json.dumps({"profiled_steps": args.ncu, "batch": batch.info(),
+                          "last_step_kernel_ms": [round(float(m), 5) for m in ms]}))
+        batch.close()
+        return
     wl, b, w0, parts, force = load_workload(args.workload, "cuda")
     params = L.make_params(dt=wl["dt"], integrator=wl["integrator"],
                            flags=L.PSF_FLAG_RENORM | (L.PSF_FLAG_FORCING if wl["force0"] else 0))
@@ -376,8 +675,11 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the FP64 accuracy/CPU baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched tensor-core form in the default line")
+    ap.add_argument("--batch-steps", type=int, default=50, help="timed steps of a batched workload")
+    ap.add_argument("--ncu-instances", type=int, default=0, help="profiling driver: only the first K instances")
     ap.add_argument("--ncu", type=int, default=0, metavar="S",
                     help="profiling driver: set up the workload, then run S steps kernel by kernel and exit")
     args = ap.parse_args()
@@ -404,7 +706,10 @@ def main():
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                               device_id=torch.device("cuda", local_rank))
     try:
-        line = run_ours(args, rank, world, local_rank)
+        if args.workload in BATCH_WORKLOADS:
+            line = run_batch_line(args, rank, world, local_rank)
+        else:
+            line = run_ours(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -44,6 +44,8 @@ typedef struct psf_batch_config {
     int32_t autotune;                /* 1: time the kernel variants at creation and keep the fastest */
     int32_t gemm_columns;            /* 0, or force the GEMM variant: 64, 128 or 256 */
     int32_t gemm_ctas;               /* 0 (one per SM), or force the persistent grid size */
+    int64_t particle_pool;           /* particles resident at once over all slots (device pool);
+                                        0 = every slot at its max_particles */
 } psf_batch_config;
 
 /* One instance placed in a slot. */
@@ -54,6 +56,7 @@ typedef struct psf_instance_desc {
     const double *forcing;    /* [n_modes] or NULL */
     const float *particles;   /* [n_particles][4] (x, y, z, life) or NULL */
     int64_t n_particles;      /* <= the basis' max_particles */
+    int32_t steps;            /* > 0: the slot stops advancing after this many steps; 0: no limit */
 } psf_instance_desc;
 
 typedef struct psf_batch psf_batch;
@@ -73,11 +76,18 @@ int psf_batch_destroy(psf_batch *b);
 int psf_batch_info_get(psf_batch *b, psf_batch_info *info);
 
 /* Place an instance in slot `slot` of basis `basis` (replaces what was there),
- * or empty the slot.  Ordered on the batch stream; returns when done. */
+ * or empty the slot.  Ordered on the batch stream; returns when done.  The
+ * instance's particles take a range of the batch's particle pool; if the
+ * pool has no free range of that size the call fails with PSF_ERR_NOMEM and
+ * the slot is left empty. */
 int psf_batch_set_instance(psf_batch *b, int32_t basis, int32_t slot, const psf_instance_desc *inst);
 int psf_batch_clear_instance(psf_batch *b, int32_t basis, int32_t slot);
 
-/* Enqueue `nsteps` steps of every occupied slot (asynchronous, graph replay). */
+/* Free particles in the pool, and the largest contiguous free range. */
+int psf_batch_pool_free(psf_batch *b, int64_t *free_particles, int64_t *largest_range);
+
+/* Enqueue `nsteps` steps of every occupied slot (asynchronous, graph replay);
+ * slots that reached their step limit do not advance. */
 int psf_batch_step(psf_batch *b, int32_t nsteps);
 int psf_batch_sync(psf_batch *b);
 int psf_batch_get_stream(psf_batch *b, void **stream);

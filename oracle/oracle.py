@@ -102,7 +102,7 @@ class OracleRollout:
     """FP64 reference-semantics rollout of one instance on a basis."""
 
     def __init__(self, b, w0, particles=None, dt=0.01, viscosity=0.0, flags=FLAG_RENORM,
-                 integrator=1, lifetime=np.inf, seed=0, forcing=None):
+                 integrator=1, lifetime=np.inf, seed=0, forcing=None, reconstruct=True):
         self.b = b
         self.N = b.n_modes
         self.C = np.ascontiguousarray(b.C, dtype=np.float64)
@@ -124,6 +124,7 @@ class OracleRollout:
         self.u = np.zeros(b.n_faces, dtype=np.float32)
         self.grid = grid_of(b)
         self.step_index = 0
+        self.reconstruct = bool(reconstruct)
         if particles is None:
             particles = np.zeros((0, 4), dtype=np.float32)
         particles = np.asarray(particles, dtype=np.float32)
@@ -135,6 +136,8 @@ class OracleRollout:
         fp = _p(self.force, ct.c_double) if self.force is not None else None
         L.psfo_coeff_step(self.N, _p(self.C, ct.c_double), _p(self.lam, ct.c_double), fp, self.dt,
                           self.visc, self.flags, _p(self.w, ct.c_double), _p(self.dw, ct.c_double))
+        if not self.reconstruct:
+            return
         L.psfo_reconstruct(self.phi.shape[0], self.N, _p(self.phi, ct.c_double),
                            _p(self.faces, ct.c_int32), self.u.shape[0], _p(self.w, ct.c_double),
                            _p(self.u, ct.c_float))

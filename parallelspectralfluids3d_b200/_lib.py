@@ -122,9 +122,10 @@ def load(path: str | None = None):
 
 def _extend(L):
     """Declare the batch and engine entry points when the build has them."""
-    from . import _lib_batch
+    from . import _lib_batch, _lib_engine
 
     _lib_batch.declare(L)
+    _lib_engine.declare(L)
 
 
 def check(rc: int) -> None:

@@ -13,7 +13,7 @@ BATCH_EXPORTS = (
     "psf_batch_create", "psf_batch_destroy", "psf_batch_info_get", "psf_batch_set_instance",
     "psf_batch_clear_instance", "psf_batch_step", "psf_batch_sync", "psf_batch_get_stream",
     "psf_batch_get_state", "psf_batch_get_particles", "psf_batch_get_velocity", "psf_batch_get_steps",
-    "psf_batch_profile_step", "psf_batch_device_status",
+    "psf_batch_profile_step", "psf_batch_device_status", "psf_batch_pool_free",
 )
 
 
@@ -33,6 +33,7 @@ class BatchConfig(ct.Structure):
         ("autotune", ct.c_int32),
         ("gemm_columns", ct.c_int32),
         ("gemm_ctas", ct.c_int32),
+        ("particle_pool", ct.c_int64),
     ]
 
 
@@ -44,6 +45,7 @@ class InstanceDesc(ct.Structure):
         ("forcing", ct.POINTER(ct.c_double)),
         ("particles", ct.POINTER(ct.c_float)),
         ("n_particles", ct.c_int64),
+        ("steps", ct.c_int32),
     ]
 
 
@@ -76,3 +78,4 @@ def declare(lib) -> None:
     lib.psf_batch_get_steps.argtypes = [vp, i32, i32, ct.POINTER(ct.c_int64)]
     lib.psf_batch_profile_step.argtypes = [vp, ct.POINTER(ct.c_double), i32]
     lib.psf_batch_device_status.argtypes = [vp, ct.POINTER(i32)]
+    lib.psf_batch_pool_free.argtypes = [vp, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]

@@ -21,7 +21,7 @@ class Batch:
     """Slots of one or more bases stepped together (BF16 hi/lo tensor-core path)."""
 
     def __init__(self, bases, slots, max_particles, device: int = 0, autotune: bool = True,
-                 gemm_columns: int = 0, gemm_ctas: int = 0):
+                 gemm_columns: int = 0, gemm_ctas: int = 0, particle_pool: int = 0):
         """``bases``: list of :class:`~.fixture.Basis`; ``slots`` / ``max_particles``: per basis (int or list)."""
         self.lib = L.load()
         n = len(bases)
@@ -44,6 +44,7 @@ class Batch:
         cfg.autotune = 1 if autotune else 0
         cfg.gemm_columns = int(gemm_columns)
         cfg.gemm_ctas = int(gemm_ctas)
+        cfg.particle_pool = int(particle_pool)
         self.handle = ct.c_void_p()
         L.check(self.lib.psf_batch_create(ct.byref(cfg), int(device), ct.byref(self.handle)))
         self._n_modes = {}
@@ -68,7 +69,8 @@ class Batch:
 
     # ---------------------------------------------------------- instances
     def set_instance(self, basis: int, slot: int, w0, params: L.Params, particles=None, forcing=None,
-                     n_modes: int | None = None) -> None:
+                     n_modes: int | None = None, steps: int = 0) -> None:
+        """Place a rollout in a slot; ``steps > 0`` stops it after that many steps."""
         w0 = np.ascontiguousarray(w0, dtype=np.float64)
         n = int(n_modes if n_modes is not None else w0.shape[0])
         d = LB.InstanceDesc()
@@ -88,6 +90,7 @@ class Batch:
             if P:
                 d.particles = L.ptr(p, ct.c_float)
         d.n_particles = P
+        d.steps = int(steps)
         L.check(self.lib.psf_batch_set_instance(self.handle, int(basis), int(slot), ct.byref(d)))
         self._n_modes[(basis, slot)] = n
         self._n_particles[(basis, slot)] = P
@@ -119,6 +122,12 @@ class Batch:
         i = LB.BatchInfo()
         L.check(self.lib.psf_batch_info_get(self.handle, ct.byref(i)))
         return {k: getattr(i, k) for k, _ in LB.BatchInfo._fields_}
+
+    def pool_free(self) -> tuple[int, int]:
+        """(free particles in the pool, largest contiguous free range)."""
+        f, l = ct.c_int64(), ct.c_int64()
+        L.check(self.lib.psf_batch_pool_free(self.handle, ct.byref(f), ct.byref(l)))
+        return int(f.value), int(l.value)
 
     def device_status(self) -> int:
         c = ct.c_int32()

@@ -69,6 +69,50 @@ int fold_signs(const psf_grid &g, const uint32_t *bits, std::vector<int8_t> &sig
     return PSF_OK;
 }
 
+void face_pair_slots(const psf_grid &g, const int32_t *faces, int64_t n_active, std::vector<int32_t> &dst)
+{
+    const int64_t nx = g.dims[0], ny = g.dims[1], nz = g.dims[2];
+    const int64_t V = nx * ny * nz;
+    const int64_t yoff = (nz + 1) * nx * ny;
+    const int64_t xoff = yoff + (ny + 1) * nx * nz;
+    dst.assign((size_t)(2 * n_active), -1);
+    auto vox = [&](int64_t x, int64_t y, int64_t z) { return z * nx * ny + y * nx + x; };
+    for (int64_t r = 0; r < n_active; ++r) {
+        const int64_t f = faces[r];
+        int64_t comp, x, y, z, lo_ok, hi_ok;
+        if (f >= xoff) {  // x-face (x in 0..nx): pair .x of voxel x, pair .y of voxel x-1
+            const int64_t t = f - xoff;
+            z = t / (ny * (nx + 1));
+            y = (t / (nx + 1)) % ny;
+            x = t % (nx + 1);
+            comp = 0;
+            lo_ok = x < nx;
+            hi_ok = x >= 1;
+            dst[2 * r] = lo_ok ? (int32_t)(2 * (comp * V + vox(x, y, z))) : -1;
+            dst[2 * r + 1] = hi_ok ? (int32_t)(2 * (comp * V + vox(x - 1, y, z)) + 1) : -1;
+        } else if (f >= yoff) {  // y-face (y in 0..ny)
+            const int64_t t = f - yoff;
+            z = t / ((ny + 1) * nx);
+            y = (t / nx) % (ny + 1);
+            x = t % nx;
+            comp = 1;
+            lo_ok = y < ny;
+            hi_ok = y >= 1;
+            dst[2 * r] = lo_ok ? (int32_t)(2 * (comp * V + vox(x, y, z))) : -1;
+            dst[2 * r + 1] = hi_ok ? (int32_t)(2 * (comp * V + vox(x, y - 1, z)) + 1) : -1;
+        } else {  // z-face (z in 0..nz)
+            z = f / (nx * ny);
+            y = (f / nx) % ny;
+            x = f % nx;
+            comp = 2;
+            lo_ok = z < nz;
+            hi_ok = z >= 1;
+            dst[2 * r] = lo_ok ? (int32_t)(2 * (comp * V + vox(x, y, z))) : -1;
+            dst[2 * r + 1] = hi_ok ? (int32_t)(2 * (comp * V + vox(x, y, z - 1)) + 1) : -1;
+        }
+    }
+}
+
 psf::GridDev make_grid_dev(const psf_grid &g)
 {
     GridDev d{};
@@ -223,7 +267,9 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     if (!b->active_faces || !b->phi || !b->advection || !b->eigenvalues || !b->sign_bits)
         return fail(PSF_ERR_INVALID, "basis arrays must not be null");
     const int64_t F = n_faces_of(g);
-    if (F >= (int64_t)UINT32_MAX) return fail(PSF_ERR_UNSUPPORTED, "grid has too many faces");
+    const int64_t V = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+    if (F >= (int64_t)UINT32_MAX || 6 * V >= (int64_t)INT32_MAX)
+        return fail(PSF_ERR_UNSUPPORTED, "grid has too many faces");
     for (int64_t r = 0; r < b->n_active; ++r)
         if (b->active_faces[r] < 0 || b->active_faces[r] >= F)
             return fail(PSF_ERR_INVALID, "active face id out of range");
@@ -278,6 +324,16 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
             (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
             (rc = c->alloc(&d.step_ctr, 1)) || (rc = c->alloc(&d.u, (size_t)F)))
             return bail(rc);
+        // Per-voxel face pairs read by the tracer, and where each active face goes.
+        std::vector<int32_t> hdst;
+        psf::face_pair_slots(g, b->active_faces, b->n_active, hdst);
+        int32_t *pdst = nullptr;
+        if ((rc = c->alloc(&d.pairs, (size_t)(3 * V))) || (rc = c->alloc(&pdst, hdst.size()))) return bail(rc);
+        d.pair_dst = pdst;
+        if ((e = cudaMemsetAsync(d.pairs, 0, (size_t)(3 * V) * sizeof(float2), c->stream)) ||
+            (e = cudaMemcpyAsync(pdst, hdst.data(), hdst.size() * 4, cudaMemcpyHostToDevice, c->stream)) ||
+            (e = cudaStreamSynchronize(c->stream)))
+            return bail(psf::cuda_fail(e, "face pair upload"));
         d.C = C;
         d.phiT = phiT;
         d.faces = faces;
@@ -297,6 +353,7 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     }
 
     d.grid = psf::make_grid_dev(g);
+    d.trace_blocks = c->num_sms * psf::trace_blocks_per_sm();
     if ((rc = apply_params(c, *params)) != PSF_OK) return bail(rc);
     *out = c;
     return PSF_OK;

@@ -143,7 +143,9 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
 // faces (4 per lane, one float4 per mode); warp g sums modes i = g (mod 8).
 __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__ phiT, long long ldp,
                                                        const int32_t *__restrict__ faces, long long n_active,
-                                                       int N, const double *__restrict__ w, float *__restrict__ u)
+                                                       int N, const double *__restrict__ w, float *__restrict__ u,
+                                                       float *__restrict__ pairs,
+                                                       const int32_t *__restrict__ pair_dst)
 {
     __shared__ float wsm[PSF_MAX_MODES];
     __shared__ float4 red[8][32];
@@ -154,9 +156,9 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (f0 < ldp) {
         const float *base = phiT + f0;
-#pragma unroll 4
+#pragma unroll 8
         for (int i = warp; i < N; i += 8) {
-            const float4 v = __ldg(reinterpret_cast<const float4 *>(base + (size_t)i * ldp));
+            const float4 v = __ldcs(reinterpret_cast<const float4 *>(base + (size_t)i * ldp));
             const float wi = wsm[i];
             acc.x = fmaf(v.x, wi, acc.x);
             acc.y = fmaf(v.y, wi, acc.y);
@@ -178,22 +180,32 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
         }
         const float vals[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (f0 + q < n_active) u[faces[f0 + q]] = vals[q];
+        for (int q = 0; q < 4; ++q) {
+            const long long r = f0 + q;
+            if (r < n_active) {
+                u[faces[r]] = vals[q];
+                const int32_t d0 = pair_dst[2 * r], d1 = pair_dst[2 * r + 1];
+                if (d0 >= 0) pairs[d0] = vals[q];
+                if (d1 >= 0) pairs[d1] = vals[q];
+            }
+        }
     }
 }
 
-__global__ void __launch_bounds__(256) psf_trace(float4 *__restrict__ parts, long long P,
+// Persistent grid (a whole number of resident blocks per SM) striding over
+// the particles, which are stored in cell order.
+__global__ void __launch_bounds__(256, 3) psf_trace(float4 *__restrict__ parts, long long P,
                                                  const int32_t *__restrict__ perm,
-                                                 const float *__restrict__ u, GridDev g, TraceParams tp,
+                                                 const float2 *__restrict__ pairs, GridDev g, TraceParams tp,
                                                  const unsigned long long *__restrict__ step_ctr)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    float4 p = parts[i];
     const uint64_t step = *step_ctr - 1ull;
-    p = advance_particle(p, g, u, tp, step, (uint32_t)perm[i]);
-    parts[i] = p;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
+        float4 p = parts[i];
+        p = advance_particle(p, g, pairs, tp, step, (uint32_t)perm[i]);
+        parts[i] = p;
+    }
 }
 
 __global__ void psf_particle_keys(const float4 *__restrict__ in, long long P, GridDev g,
@@ -285,16 +297,25 @@ int launch_contract_state(const PlainDev &d, cudaStream_t st)
 int launch_reconstruct(const PlainDev &d, cudaStream_t st)
 {
     const long long blocks = (d.n_active + 127) / 128;
-    psf_reconstruct<<<(unsigned)blocks, 256, 0, st>>>(d.phiT, d.ldp, d.faces, d.n_active, d.N, d.w, d.u);
+    psf_reconstruct<<<(unsigned)blocks, 256, 0, st>>>(d.phiT, d.ldp, d.faces, d.n_active, d.N, d.w, d.u,
+                                                      reinterpret_cast<float *>(d.pairs), d.pair_dst);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_reconstruct launch");
+}
+
+int trace_blocks_per_sm()
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_trace, 256, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 4;
+    return per_sm;
 }
 
 int launch_trace(const PlainDev &d, cudaStream_t st)
 {
     if (d.P == 0) return PSF_OK;
-    const long long blocks = (d.P + 255) / 256;
-    psf_trace<<<(unsigned)blocks, 256, 0, st>>>(d.parts, d.P, d.perm, d.u, d.grid, d.tp, d.step_ctr);
+    const long long blocks = std::min<long long>((d.P + 255) / 256, std::max(1, d.trace_blocks));
+    psf_trace<<<(unsigned)blocks, 256, 0, st>>>(d.parts, d.P, d.perm, d.pairs, d.grid, d.tp, d.step_ctr);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_trace launch");
 }

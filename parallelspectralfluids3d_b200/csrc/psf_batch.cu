@@ -236,11 +236,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
                         G.dwpart[((size_t)(outer * G.m_inner + inner) * 4 + q) * G.cap + b] = s;
                 }
             } else {
-                // Face velocities of this warp's 32 rows, scattered to the
-                // reference face numbering of every slot's field.
+                // Face velocities of this warp's 32 rows, scattered into every
+                // slot's per-voxel face pairs (each face lands in its two voxels).
                 const long long f = (long long)inner * 128 + row;
                 const bool frow = f < G.n_rows;
-                const long long face = frow ? (long long)__ldg(G.faces + f) : 0;
+                const int32_t d0 = frow ? __ldg(G.pair_dst + 2 * f) : -1;
+                const int32_t d1 = frow ? __ldg(G.pair_dst + 2 * f + 1) : -1;
                 for (int c0 = 0; c0 < G.bn; c0 += 32) {
                     float y[32];
                     tmem_ld32(tbase + (uint32_t)c0, y);
@@ -248,7 +249,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
 #pragma unroll
                         for (int c = 0; c < 32; ++c) {
                             const int b = c0 + c;
-                            if (b < G.cap) G.u[(size_t)b * G.n_faces + face] = y[c];
+                            if (b < G.cap) {
+                                float *pr = G.pairs + (size_t)b * G.pair_floats;
+                                if (d0 >= 0) pr[d0] = y[c];
+                                if (d1 >= 0) pr[d1] = y[c];
+                            }
                         }
                     }
                 }
@@ -287,6 +292,10 @@ __global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restric
     __shared__ double wnew[PSF_MAX_MODES];
     SlotDev &s = slots[blockIdx.x];
     if (!s.active) return;
+    if (s.target != 0ull && s.step >= s.target) {
+        if (threadIdx.x == 0) s.stepped = 0;
+        return;
+    }
     const GroupDev &G = groups[s.group];
     const int b = s.slot, N = s.n_modes, at = G.a_tiles, cap = G.cap;
     double *w = G.w + (size_t)b * G.N;
@@ -314,7 +323,10 @@ __global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restric
         w[i] = v;
         split_bf16(v, Whi + i, Wlo + i);
     }
-    if (threadIdx.x == 0) s.step += 1ull;
+    if (threadIdx.x == 0) {
+        s.step += 1ull;
+        s.stepped = 1;
+    }
 }
 
 // BF16 split of one slot's current state (after it was set from the host).
@@ -331,7 +343,7 @@ __global__ void psf_batch_pack(const GroupDev *__restrict__ groups, const SlotDe
 }
 
 // ------------------------------------------------------------------ tracer
-__global__ void __launch_bounds__(256) psf_batch_trace(const GroupDev *__restrict__ groups,
+__global__ void __launch_bounds__(256, 3) psf_batch_trace(const GroupDev *__restrict__ groups,
                                                        const SlotDev *__restrict__ slots,
                                                        const TraceItem *__restrict__ items,
                                                        const int *__restrict__ n_items)
@@ -341,15 +353,16 @@ __global__ void __launch_bounds__(256) psf_batch_trace(const GroupDev *__restric
         const TraceItem ti = items[it];
         if ((int)threadIdx.x >= ti.count) continue;
         const SlotDev &s = slots[ti.slot_global];
+        if (!s.stepped) continue;
         const GroupDev &G = groups[s.group];
-        const size_t idx = (size_t)s.slot * (size_t)G.pmax + (size_t)ti.start + threadIdx.x;
+        const size_t idx = (size_t)s.poff + (size_t)ti.start + threadIdx.x;
         TraceParams tp;
         tp.dt = (float)s.dt;
         tp.lifetime = s.lifetime;
         tp.rk4 = s.rk4;
         tp.seed = s.seed;
         float4 p = G.parts[idx];
-        p = advance_particle(p, G.grid, G.u + (size_t)s.slot * (size_t)G.n_faces, tp, s.step - 1ull,
+        p = advance_particle(p, G.grid, G.pairs + (size_t)s.slot * 3 * (size_t)G.V, tp, s.step - 1ull,
                              (uint32_t)G.perm[idx]);
         G.parts[idx] = p;
     }

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 #include <vector>
@@ -47,12 +48,73 @@ struct HostGroup {
     uint16_t *C = nullptr;    // BF16 [N][2][Na][Nj]
     uint16_t *Phi = nullptr;  // BF16 [2][Fp][Nj]
     uint16_t *W = nullptr;    // BF16 [2][bn][Nj]
-    int32_t *faces = nullptr;
     double *lam = nullptr, *w = nullptr, *force = nullptr, *dwpart = nullptr;
-    float *u = nullptr;
-    float4 *parts = nullptr;
-    int32_t *perm = nullptr;
+    float2 *pairs = nullptr;
+    std::vector<int32_t> faces_host, dst_host;  // for reading a slot's face field back
+    int32_t *pair_dst = nullptr;
+    int64_t V = 0;
     CUtensorMap mapC{}, mapPhi{}, mapW{};
+};
+
+// First-fit allocator of particle ranges in the batch's device pool, in
+// units of 256 particles (one tracer work item).
+class RangePool {
+public:
+    void reset(int64_t units)
+    {
+        free_.clear();
+        total_ = units;
+        if (units > 0) free_[0] = units;
+    }
+    bool alloc(int64_t units, int64_t *start)
+    {
+        if (units == 0) {
+            *start = 0;
+            return true;
+        }
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= units) {
+                *start = it->first;
+                const int64_t rest = it->second - units, at = it->first + units;
+                free_.erase(it);
+                if (rest > 0) free_[at] = rest;
+                return true;
+            }
+        return false;
+    }
+    void release(int64_t start, int64_t units)
+    {
+        if (units == 0) return;
+        auto it = free_.emplace(start, units).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    int64_t free_units() const
+    {
+        int64_t n = 0;
+        for (const auto &r : free_) n += r.second;
+        return n;
+    }
+    int64_t largest() const
+    {
+        int64_t n = 0;
+        for (const auto &r : free_) n = std::max(n, r.second);
+        return n;
+    }
+
+private:
+    std::map<int64_t, int64_t> free_;
+    int64_t total_ = 0;
 };
 
 }  // namespace
@@ -80,6 +142,11 @@ struct psf_batch {
     double tuned_ms = 0.0;
     psf::OrderBufs order{};
     int64_t pmax_all = 0;
+    float4 *pool_parts = nullptr;   // particle pool shared by all slots
+    int32_t *pool_perm = nullptr;
+    int64_t pool_cap = 0;           // particles
+    RangePool pool;
+    std::vector<int64_t> slot_units;  // pool units held by each slot
     int64_t bytes = 0;
     std::vector<void *> allocs;
 
@@ -145,9 +212,7 @@ int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
         PSF_CUDA(cudaMemcpyAsync(G.Phi, h.data(), h.size() * 2, cudaMemcpyHostToDevice, st));
         PSF_CUDA(cudaStreamSynchronize(st));
     }
-    PSF_CHECK(B->alloc(&G.faces, (size_t)G.F_act));
     PSF_CHECK(B->alloc(&G.lam, (size_t)N));
-    PSF_CUDA(cudaMemcpyAsync(G.faces, b.active_faces, (size_t)G.F_act * 4, cudaMemcpyHostToDevice, st));
     PSF_CUDA(cudaMemcpyAsync(G.lam, b.eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st));
 
     const size_t cap = (size_t)G.cap;
@@ -155,14 +220,17 @@ int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
     PSF_CHECK(B->alloc(&G.w, cap * N));
     PSF_CHECK(B->alloc(&G.force, cap * N));
     PSF_CHECK(B->alloc(&G.dwpart, (size_t)N * G.a_tiles * 4 * cap));
-    PSF_CHECK(B->alloc(&G.u, cap * (size_t)G.n_faces));
-    PSF_CHECK(B->alloc(&G.parts, cap * (size_t)G.pmax));
-    PSF_CHECK(B->alloc(&G.perm, cap * (size_t)G.pmax));
+    G.faces_host.assign(b.active_faces, b.active_faces + G.F_act);
+    psf::face_pair_slots(G.grid, b.active_faces, G.F_act, G.dst_host);
+    PSF_CHECK(B->alloc(&G.pair_dst, G.dst_host.size()));
+    PSF_CUDA(cudaMemcpyAsync(G.pair_dst, G.dst_host.data(), G.dst_host.size() * 4, cudaMemcpyHostToDevice, st));
+    PSF_CUDA(cudaStreamSynchronize(st));
+    PSF_CHECK(B->alloc(&G.pairs, cap * (size_t)(3 * G.V)));
+    PSF_CUDA(cudaMemsetAsync(G.pairs, 0, cap * (size_t)(3 * G.V) * sizeof(float2), st));
     PSF_CUDA(cudaMemsetAsync(G.W, 0, (size_t)2 * G.bn * G.Nj * 2, st));
     PSF_CUDA(cudaMemsetAsync(G.w, 0, cap * N * 8, st));
     PSF_CUDA(cudaMemsetAsync(G.force, 0, cap * N * 8, st));
     PSF_CUDA(cudaMemsetAsync(G.dwpart, 0, (size_t)N * G.a_tiles * 4 * cap * 8, st));
-    PSF_CUDA(cudaMemsetAsync(G.u, 0, cap * (size_t)G.n_faces * 4, st));
 
     // Tensor maps: inner dimension first, strides in bytes for dims 1..
     {
@@ -222,9 +290,10 @@ void fill_gemm_args(psf_batch *B)
         y.cap = G.cap;
         y.n_rows = (int)G.F_act;
         y.ldw = G.N;
-        y.faces = G.faces;
-        y.u = G.u;
         y.n_faces = G.n_faces;
+        y.pair_dst = G.pair_dst;
+        y.pairs = reinterpret_cast<float *>(G.pairs);
+        y.pair_floats = 6 * G.V;
         r.total_tiles += y.tiles;
     }
 }
@@ -249,9 +318,10 @@ int upload_tables(psf_batch *B)
         d.lam = G.lam;
         d.dwpart = G.dwpart;
         d.W = G.W;
-        d.u = G.u;
-        d.parts = G.parts;
-        d.perm = G.perm;
+        d.pairs = G.pairs;
+        d.V = G.V;
+        d.parts = B->pool_parts;
+        d.perm = B->pool_perm;
     }
     PSF_CUDA(cudaMemcpyAsync(B->d_groups, gd.data(), gd.size() * sizeof(psf::GroupDev), cudaMemcpyHostToDevice,
                              B->stream));
@@ -378,11 +448,12 @@ int slot_index(psf_batch *B, int32_t basis, int32_t slot, int *sg)
 psf::PlainDev particle_view(psf_batch *B, int basis, int slot, int64_t count)
 {
     HostGroup &G = B->groups[(size_t)basis];
+    const psf::SlotDev &s = B->slots[(size_t)(G.slot_base + slot)];
     psf::PlainDev d{};
     d.grid = psf::make_grid_dev(G.grid);
     d.P = count;
-    d.parts = G.parts + (size_t)slot * G.pmax;
-    d.perm = G.perm + (size_t)slot * G.pmax;
+    d.parts = B->pool_parts + s.poff;
+    d.perm = B->pool_perm + s.poff;
     return d;
 }
 
@@ -415,7 +486,9 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
         if (b.grid.dims[0] == 0 || b.grid.dims[1] == 0 || b.grid.dims[2] == 0 || !(b.grid.resolution > 0.0))
             return fail(PSF_ERR_INVALID, "grid dims and resolution must be positive");
         const int64_t F = psf::n_faces_of(b.grid);
-        if (F >= (int64_t)INT32_MAX) return fail(PSF_ERR_UNSUPPORTED, "grid has too many faces");
+        const int64_t V = (int64_t)b.grid.dims[0] * b.grid.dims[1] * b.grid.dims[2];
+        if (F >= (int64_t)INT32_MAX || 6 * V >= (int64_t)INT32_MAX)
+            return fail(PSF_ERR_UNSUPPORTED, "grid has too many faces");
         for (int64_t r = 0; r < b.n_active; ++r)
             if (b.active_faces[r] < 0 || b.active_faces[r] >= F)
                 return fail(PSF_ERR_INVALID, "active face id out of range");
@@ -462,6 +535,7 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
             G.Fp = round_up(G.F_act, 128);
             G.grid = bb.basis.grid;
             G.n_faces = psf::n_faces_of(G.grid);
+            G.V = (int64_t)G.grid.dims[0] * G.grid.dims[1] * G.grid.dims[2];
             G.pmax = round_up(std::max<int64_t>(1, bb.max_particles), 256);
             B->pmax_all = std::max(B->pmax_all, G.pmax);
             slot_base += G.cap;
@@ -478,8 +552,17 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
     } catch (const std::bad_alloc &) {
         return bail(fail(PSF_ERR_NOMEM, "host staging allocation failed"));
     }
-    for (const HostGroup &G : B->groups) B->item_cap += (int64_t)G.cap * (G.pmax / 256);
-    if ((rc = B->alloc(&B->d_groups, B->groups.size())) || (rc = B->alloc(&B->d_slots, B->slots.size())) ||
+    {
+        int64_t all_slots = 0;
+        for (const HostGroup &G : B->groups) all_slots += (int64_t)G.cap * G.pmax;
+        B->pool_cap = cfg->particle_pool > 0 ? round_up(cfg->particle_pool, 256) : all_slots;
+        if (B->pool_cap > (int64_t)INT32_MAX) return bail(fail(PSF_ERR_UNSUPPORTED, "particle pool too large"));
+        B->pool.reset(B->pool_cap / 256);
+        B->slot_units.assign((size_t)slot_base, 0);
+        B->item_cap = B->pool_cap / 256 + slot_base;
+    }
+    if ((rc = B->alloc(&B->pool_parts, (size_t)B->pool_cap)) || (rc = B->alloc(&B->pool_perm, (size_t)B->pool_cap)) ||
+        (rc = B->alloc(&B->d_groups, B->groups.size())) || (rc = B->alloc(&B->d_slots, B->slots.size())) ||
         (rc = B->alloc(&B->d_items, (size_t)B->item_cap)) || (rc = B->alloc(&B->d_n_items, 1)))
         return bail(rc);
     // Particle ordering scratch, sized for the largest slot.
@@ -549,15 +632,35 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
         return fail(PSF_ERR_INVALID, "integrator must be PSF_RK1 or PSF_RK4");
     if ((p.flags & PSF_FLAG_FORCING) && !inst->forcing)
         return fail(PSF_ERR_INVALID, "PSF_FLAG_FORCING is set but forcing is null");
+    if (inst->steps < 0) return fail(PSF_ERR_INVALID, "steps must be >= 0");
     PSF_CUDA(cudaSetDevice(B->device));
     cudaStream_t st = B->stream;
+    // Particle range: give back the slot's old one, then take a new one.
+    psf::SlotDev &s = B->slots[(size_t)sg];
+    if (B->slot_units[(size_t)sg] > 0) {
+        PSF_CUDA(cudaStreamSynchronize(st));
+        B->pool.release(s.poff / 256, B->slot_units[(size_t)sg]);
+        B->slot_units[(size_t)sg] = 0;
+    }
+    const int64_t units = (inst->n_particles + 255) / 256;
+    int64_t start = 0;
+    if (!B->pool.alloc(units, &start)) {
+        s.active = 0;
+        s.n_particles = 0;
+        PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, st));
+        PSF_CHECK(upload_items(B));
+        return fail(PSF_ERR_NOMEM, "the particle pool has no free range for this instance");
+    }
+    B->slot_units[(size_t)sg] = units;
     std::vector<double> row((size_t)G.N, 0.0), frow((size_t)G.N, 0.0);
     std::memcpy(row.data(), inst->w0, (size_t)inst->n_modes * 8);
     if (inst->forcing) std::memcpy(frow.data(), inst->forcing, (size_t)inst->n_modes * 8);
     PSF_CUDA(cudaMemcpyAsync(G.w + (size_t)slot * G.N, row.data(), row.size() * 8, cudaMemcpyHostToDevice, st));
     PSF_CUDA(cudaMemcpyAsync(G.force + (size_t)slot * G.N, frow.data(), frow.size() * 8, cudaMemcpyHostToDevice, st));
-    psf::SlotDev &s = B->slots[(size_t)sg];
     s.active = 1;
+    s.poff = start * 256;
+    s.target = (unsigned long long)inst->steps;
+    s.stepped = 0;
     s.n_modes = inst->n_modes;
     s.rk4 = p.integrator == PSF_RK4;
     s.flags = p.flags;
@@ -586,12 +689,26 @@ int psf_batch_clear_instance(psf_batch *B, int32_t basis, int32_t slot)
     PSF_CUDA(cudaSetDevice(B->device));
     HostGroup &G = B->groups[(size_t)basis];
     psf::SlotDev &s = B->slots[(size_t)sg];
+    if (B->slot_units[(size_t)sg] > 0) {
+        PSF_CUDA(cudaStreamSynchronize(B->stream));
+        B->pool.release(s.poff / 256, B->slot_units[(size_t)sg]);
+        B->slot_units[(size_t)sg] = 0;
+    }
     s.active = 0;
     s.n_particles = 0;
+    s.stepped = 0;
     PSF_CUDA(cudaMemsetAsync(G.w + (size_t)slot * G.N, 0, (size_t)G.N * 8, B->stream));
     PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, B->stream));
     PSF_CHECK(psf::launch_batch_pack(B->d_groups, B->d_slots, sg, B->stream));
     PSF_CHECK(upload_items(B));
+    return PSF_OK;
+}
+
+int psf_batch_pool_free(psf_batch *B, int64_t *free_particles, int64_t *largest_range)
+{
+    if (!B || !free_particles || !largest_range) return fail(PSF_ERR_INVALID, "null argument");
+    *free_particles = B->pool.free_units() * 256;
+    *largest_range = B->pool.largest() * 256;
     return PSF_OK;
 }
 
@@ -658,10 +775,23 @@ int psf_batch_get_velocity(psf_batch *B, int32_t basis, int32_t slot, float *u, 
     if (!u) return fail(PSF_ERR_INVALID, "null argument");
     if (n_faces != G.n_faces) return fail(PSF_ERR_INVALID, "n_faces must equal the grid's face count");
     PSF_CUDA(cudaSetDevice(B->device));
-    PSF_CUDA(cudaMemcpyAsync(u, G.u + (size_t)slot * G.n_faces, (size_t)n_faces * 4, cudaMemcpyDeviceToHost,
+    // The slot's field lives in its per-voxel face pairs; every active face is
+    // stored in both adjacent voxels, wall faces are zero.
+    std::vector<float> pf;
+    try {
+        pf.resize((size_t)(6 * G.V));
+    } catch (const std::bad_alloc &) {
+        return fail(PSF_ERR_NOMEM, "host staging allocation failed");
+    }
+    PSF_CUDA(cudaMemcpyAsync(pf.data(), G.pairs + (size_t)slot * 3 * G.V, pf.size() * 4, cudaMemcpyDeviceToHost,
                              B->stream));
     PSF_CUDA(cudaStreamSynchronize(B->stream));
-    for (int64_t f = 0; f < n_faces; ++f) u[f] *= (float)G.sigma[(size_t)f];
+    std::fill(u, u + n_faces, 0.f);
+    for (int64_t r = 0; r < G.F_act; ++r) {
+        const int32_t face = G.faces_host[(size_t)r];
+        const int32_t d = G.dst_host[(size_t)(2 * r)] >= 0 ? G.dst_host[(size_t)(2 * r)] : G.dst_host[(size_t)(2 * r + 1)];
+        if (d >= 0) u[face] = pf[(size_t)d] * (float)G.sigma[(size_t)face];
+    }
     return check_device_error(B);
 }
 

@@ -31,9 +31,10 @@ struct alignas(64) GemmGroup {
     int ldw;                // row stride of w (= the basis' N)
     const double *w;        // contraction: FP64 state [cap][ldw]
     double *dwpart;         // contraction: partials [((k*m_inner + at)*4 + q)][cap]
-    const int32_t *faces;   // reconstruction: reference face id of each row
-    float *u;               // reconstruction: face field [cap][n_faces]
     long long n_faces;
+    const int32_t *pair_dst;  // reconstruction: [n_rows][2] float slots in a slot's face pairs
+    float *pairs;           // reconstruction: per-voxel face pairs [cap][3V] (float2)
+    long long pair_floats;  // 6V: floats per slot in pairs
 };
 
 struct GemmArgs {
@@ -58,6 +59,10 @@ struct SlotDev {
     unsigned long long seed;
     unsigned long long step;  // steps taken since the slot was set (device counter)
     long long n_particles;
+    long long poff;           // first particle of the slot in the particle pool
+    unsigned long long target;  // stop after this many steps (0: no limit)
+    int stepped;              // 1 if the slot advanced in the current step (set by the state kernel)
+    int pad1;
 };
 
 // Per-basis device view used by the state kernel and the tracer.
@@ -70,9 +75,10 @@ struct GroupDev {
     const double *lam;    // [N]
     double *dwpart;       // see GemmGroup
     uint16_t *W;          // BF16 [2][bn][Nj]
-    float *u;             // [cap][n_faces]
-    float4 *parts;        // [cap][pmax]
-    int32_t *perm;        // [cap][pmax]
+    float2 *pairs;        // [cap][3V] per-voxel face pairs of each slot
+    long long V;
+    float4 *parts;        // particle pool (all slots of the batch)
+    int32_t *perm;        // caller index of each pooled particle
 };
 
 // One tracer work item: up to 256 particles of one slot.

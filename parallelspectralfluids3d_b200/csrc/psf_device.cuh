@@ -16,19 +16,6 @@ namespace psf {
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 __device__ __forceinline__ float mixf(float x, float y, float a) { return x * (1.f - a) + y * a; }
 
-__device__ __forceinline__ uint32_t zface(const GridDev &g, int x, int y, int z)
-{
-    return (uint32_t)z * (uint32_t)(g.nx * g.ny) + (uint32_t)(y * g.nx + x);
-}
-__device__ __forceinline__ uint32_t yface(const GridDev &g, int x, int y, int z)
-{
-    return (uint32_t)z * (uint32_t)((g.ny + 1) * g.nx) + (uint32_t)(y * g.nx + x) + g.yoff;
-}
-__device__ __forceinline__ uint32_t xface(const GridDev &g, int x, int y, int z)
-{
-    return (uint32_t)z * (uint32_t)(g.ny * (g.nx + 1)) + (uint32_t)(y * (g.nx + 1) + x) + g.xoff;
-}
-
 // Counter-based generator for respawns (SplitMix64 output function); the
 // oracle uses the same function so respawns are reproducible.
 __host__ __device__ __forceinline__ uint32_t respawn_hash(uint64_t seed, uint64_t step, uint32_t idx,
@@ -65,60 +52,124 @@ __device__ inline double block_sum_256(double v, double *red)
     return t;
 }
 
-// --------------------------------------------------------- 3. tracing
-// Staggered trilinear interpolation (psfsolver.cpp:80-212): for each
-// component, eight face samples mixed along y, then x, then z.  The face
-// field is already signed, so no sign-string lookups are needed.
-__device__ __forceinline__ float3 velocity_at(const GridDev &g, const float *__restrict__ u, float px, float py,
-                                              float pz)
+// ------------------------------------------------------------------ tracing
+// The tracer reads the face field through a per-voxel copy ("face pairs"):
+// for voxel v, pairs[v] = (u of its x-face at x, at x+1), pairs[V + v] the
+// same for y, pairs[2V + v] for z, already carrying the tracer's face signs.
+// One trilinear component then needs four aligned float2 loads instead of
+// eight scalar gathers.  The interpolant is the reference's
+// (psfsolver.cpp:80-212): clamped staggered cell indices, eight face samples
+// per component mixed along y, then x, then z, weights not clamped.
+__device__ __forceinline__ uint32_t voxel(const GridDev &g, int x, int y, int z)
+{
+    return (uint32_t)z * (uint32_t)(g.nx * g.ny) + (uint32_t)(y * g.nx + x);
+}
+
+// Staggered cell of a position: the clamped voxel indices of the three
+// component stencils, and the position in voxel units from the box corner.
+struct Cell {
+    int xO, yO, zO, xM, xP, yM, yP, zM, zP;
+};
+
+__device__ __forceinline__ Cell cell_of(const GridDev &g, float px, float py, float pz, float3 &gw)
 {
     const float gix = (g.shift[0] + px) * g.inv_h;
     const float giy = (g.shift[1] + py) * g.inv_h;
     const float giz = (g.shift[2] + pz) * g.inv_h;
-    const float gwx = (px - g.mn[0]) * g.inv_h;
-    const float gwy = (py - g.mn[1]) * g.inv_h;
-    const float gwz = (pz - g.mn[2]) * g.inv_h;
-    const int xO = clampi((int)floorf(gix), 0, g.nx - 1);
-    const int yO = clampi((int)floorf(giy), 0, g.ny - 1);
-    const int zO = clampi((int)floorf(giz), 0, g.nz - 1);
+    gw.x = (px - g.mn[0]) * g.inv_h;
+    gw.y = (py - g.mn[1]) * g.inv_h;
+    gw.z = (pz - g.mn[2]) * g.inv_h;
+    Cell c;
+    c.xO = clampi((int)floorf(gix), 0, g.nx - 1);
+    c.yO = clampi((int)floorf(giy), 0, g.ny - 1);
+    c.zO = clampi((int)floorf(giz), 0, g.nz - 1);
     const int xr = (int)floorf(gix - 0.5f), yr = (int)floorf(giy - 0.5f), zr = (int)floorf(giz - 0.5f);
-    const int xM = clampi(xr, 0, g.nx - 1), xP = clampi(xr + 1, 0, g.nx - 1);
-    const int yM = clampi(yr, 0, g.ny - 1), yP = clampi(yr + 1, 0, g.ny - 1);
-    const int zM = clampi(zr, 0, g.nz - 1), zP = clampi(zr + 1, 0, g.nz - 1);
+    c.xM = clampi(xr, 0, g.nx - 1);
+    c.xP = clampi(xr + 1, 0, g.nx - 1);
+    c.yM = clampi(yr, 0, g.ny - 1);
+    c.yP = clampi(yr + 1, 0, g.ny - 1);
+    c.zM = clampi(zr, 0, g.nz - 1);
+    c.zP = clampi(zr + 1, 0, g.nz - 1);
+    return c;
+}
+
+__device__ __forceinline__ bool same_cell(const Cell &a, const Cell &b)
+{
+    return a.xO == b.xO && a.yO == b.yO && a.zO == b.zO && a.xM == b.xM && a.xP == b.xP && a.yM == b.yM &&
+           a.yP == b.yP && a.zM == b.zM && a.zP == b.zP;
+}
+
+// The 24 face samples of a cell as 12 face pairs.
+struct CellSamples {
+    float2 x00, x10, x01, x11;  // x-face pairs at (xO, yM|yP, zM|zP)
+    float2 yM0, yP0, yM1, yP1;  // y-face pairs at (xM|xP, yO, zM|zP)
+    float2 zMM, zMP, zPM, zPP;  // z-face pairs at (xM|xP, yM|yP, zO)
+};
+
+__device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, const Cell &c,
+                                            CellSamples &s)
+{
+    const uint32_t V = (uint32_t)g.nx * (uint32_t)g.ny * (uint32_t)g.nz;
+    const float2 *__restrict__ pxp = pairs;
+    const float2 *__restrict__ pyp = pairs + V;
+    const float2 *__restrict__ pzp = pairs + 2 * (size_t)V;
+    s.x00 = __ldg(pxp + voxel(g, c.xO, c.yM, c.zM));
+    s.x10 = __ldg(pxp + voxel(g, c.xO, c.yP, c.zM));
+    s.x01 = __ldg(pxp + voxel(g, c.xO, c.yM, c.zP));
+    s.x11 = __ldg(pxp + voxel(g, c.xO, c.yP, c.zP));
+    s.yM0 = __ldg(pyp + voxel(g, c.xM, c.yO, c.zM));
+    s.yP0 = __ldg(pyp + voxel(g, c.xP, c.yO, c.zM));
+    s.yM1 = __ldg(pyp + voxel(g, c.xM, c.yO, c.zP));
+    s.yP1 = __ldg(pyp + voxel(g, c.xP, c.yO, c.zP));
+    s.zMM = __ldg(pzp + voxel(g, c.xM, c.yM, c.zO));
+    s.zMP = __ldg(pzp + voxel(g, c.xM, c.yP, c.zO));
+    s.zPM = __ldg(pzp + voxel(g, c.xP, c.yM, c.zO));
+    s.zPP = __ldg(pzp + voxel(g, c.xP, c.yP, c.zO));
+}
+
+__device__ __forceinline__ float3 interpolate(const Cell &c, const CellSamples &s, const float3 &gw)
+{
     float3 v;
     {  // x: faces (xO | xO+1, yM | yP, zM | zP)
-        const float tx = gwx - (float)xO, ty = gwy - ((float)yM + 0.5f), tz = gwz - ((float)zM + 0.5f);
-        const uint32_t i00 = xface(g, xO, yM, zM), i10 = xface(g, xO, yP, zM);
-        const uint32_t i01 = xface(g, xO, yM, zP), i11 = xface(g, xO, yP, zP);
-        const float a = mixf(__ldg(u + i00), __ldg(u + i10), ty);
-        const float b = mixf(__ldg(u + i00 + 1), __ldg(u + i10 + 1), ty);
-        const float c = mixf(__ldg(u + i01), __ldg(u + i11), ty);
-        const float d = mixf(__ldg(u + i01 + 1), __ldg(u + i11 + 1), ty);
-        v.x = mixf(mixf(a, b, tx), mixf(c, d, tx), tz);
+        const float tx = gw.x - (float)c.xO, ty = gw.y - ((float)c.yM + 0.5f), tz = gw.z - ((float)c.zM + 0.5f);
+        const float a = mixf(s.x00.x, s.x10.x, ty);
+        const float b = mixf(s.x00.y, s.x10.y, ty);
+        const float cc = mixf(s.x01.x, s.x11.x, ty);
+        const float d = mixf(s.x01.y, s.x11.y, ty);
+        v.x = mixf(mixf(a, b, tx), mixf(cc, d, tx), tz);
     }
     {  // y: faces (xM | xP, yO | yO+1, zM | zP)
-        const float tx = gwx - ((float)xM + 0.5f), ty = gwy - (float)yO, tz = gwz - ((float)zM + 0.5f);
-        const uint32_t iM0 = yface(g, xM, yO, zM), iP0 = yface(g, xP, yO, zM);
-        const uint32_t iM1 = yface(g, xM, yO, zP), iP1 = yface(g, xP, yO, zP);
-        const uint32_t up = (uint32_t)g.nx;  // yO + 1
-        const float a = mixf(__ldg(u + iM0), __ldg(u + iM0 + up), ty);
-        const float b = mixf(__ldg(u + iP0), __ldg(u + iP0 + up), ty);
-        const float c = mixf(__ldg(u + iM1), __ldg(u + iM1 + up), ty);
-        const float d = mixf(__ldg(u + iP1), __ldg(u + iP1 + up), ty);
-        v.y = mixf(mixf(a, b, tx), mixf(c, d, tx), tz);
+        const float tx = gw.x - ((float)c.xM + 0.5f), ty = gw.y - (float)c.yO, tz = gw.z - ((float)c.zM + 0.5f);
+        const float a = mixf(s.yM0.x, s.yM0.y, ty);
+        const float b = mixf(s.yP0.x, s.yP0.y, ty);
+        const float cc = mixf(s.yM1.x, s.yM1.y, ty);
+        const float d = mixf(s.yP1.x, s.yP1.y, ty);
+        v.y = mixf(mixf(a, b, tx), mixf(cc, d, tx), tz);
     }
     {  // z: faces (xM | xP, yM | yP, zO | zO+1)
-        const float tx = gwx - ((float)xM + 0.5f), ty = gwy - ((float)yM + 0.5f), tz = gwz - (float)zO;
-        const uint32_t iMM = zface(g, xM, yM, zO), iMP = zface(g, xM, yP, zO);
-        const uint32_t iPM = zface(g, xP, yM, zO), iPP = zface(g, xP, yP, zO);
-        const uint32_t up = (uint32_t)(g.nx * g.ny);  // zO + 1
-        const float a = mixf(__ldg(u + iMM), __ldg(u + iMP), ty);
-        const float b = mixf(__ldg(u + iPM), __ldg(u + iPP), ty);
-        const float c = mixf(__ldg(u + iMM + up), __ldg(u + iMP + up), ty);
-        const float d = mixf(__ldg(u + iPM + up), __ldg(u + iPP + up), ty);
-        v.z = mixf(mixf(a, b, tx), mixf(c, d, tx), tz);
+        const float tx = gw.x - ((float)c.xM + 0.5f), ty = gw.y - ((float)c.yM + 0.5f), tz = gw.z - (float)c.zO;
+        const float a = mixf(s.zMM.x, s.zMP.x, ty);
+        const float b = mixf(s.zPM.x, s.zPP.x, ty);
+        const float cc = mixf(s.zMM.y, s.zMP.y, ty);
+        const float d = mixf(s.zPM.y, s.zPP.y, ty);
+        v.z = mixf(mixf(a, b, tx), mixf(cc, d, tx), tz);
     }
     return v;
+}
+
+// Velocity at a position; `c`/`s` carry the last gathered cell, and the
+// samples are loaded again only when the position lies in another cell.
+__device__ __forceinline__ float3 velocity_cached(const GridDev &g, const float2 *__restrict__ pairs, float px,
+                                                  float py, float pz, Cell &c, CellSamples &s, bool &have)
+{
+    float3 gw;
+    const Cell n = cell_of(g, px, py, pz, gw);
+    if (!have || !same_cell(n, c)) {
+        c = n;
+        gather_cell(g, pairs, c, s);
+        have = true;
+    }
+    return interpolate(c, s, gw);
 }
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
@@ -127,31 +178,34 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fm
 // on every stage, lifetime decrement, and respawn from the counter-based
 // generator keyed by the caller-order index `id` when the lifetime ran out.
 // `step` is the index of the step being taken (0 for the first).
-__device__ __forceinline__ float4 advance_particle(float4 p, const GridDev &g, const float *__restrict__ u,
+__device__ __forceinline__ float4 advance_particle(float4 p, const GridDev &g, const float2 *__restrict__ u,
                                                    const TraceParams &tp, uint64_t step, uint32_t id)
 {
     if (p.w > 0.f) {
         const float dt = tp.dt;
+        Cell c;
+        CellSamples cs;
+        bool have = false;
         float3 v;
         if (tp.rk4) {
-            const float3 k1 = velocity_at(g, u, p.x, p.y, p.z);
+            const float3 k1 = velocity_cached(g, u, p.x, p.y, p.z, c, cs, have);
             float qx = clampf(p.x + 0.5f * dt * k1.x, g.mn[0], g.mx[0]);
             float qy = clampf(p.y + 0.5f * dt * k1.y, g.mn[1], g.mx[1]);
             float qz = clampf(p.z + 0.5f * dt * k1.z, g.mn[2], g.mx[2]);
-            const float3 k2 = velocity_at(g, u, qx, qy, qz);
+            const float3 k2 = velocity_cached(g, u, qx, qy, qz, c, cs, have);
             qx = clampf(p.x + 0.5f * dt * k2.x, g.mn[0], g.mx[0]);
             qy = clampf(p.y + 0.5f * dt * k2.y, g.mn[1], g.mx[1]);
             qz = clampf(p.z + 0.5f * dt * k2.z, g.mn[2], g.mx[2]);
-            const float3 k3 = velocity_at(g, u, qx, qy, qz);
+            const float3 k3 = velocity_cached(g, u, qx, qy, qz, c, cs, have);
             qx = clampf(p.x + dt * k3.x, g.mn[0], g.mx[0]);
             qy = clampf(p.y + dt * k3.y, g.mn[1], g.mx[1]);
             qz = clampf(p.z + dt * k3.z, g.mn[2], g.mx[2]);
-            const float3 k4 = velocity_at(g, u, qx, qy, qz);
+            const float3 k4 = velocity_cached(g, u, qx, qy, qz, c, cs, have);
             v.x = (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x) / 6.f;
             v.y = (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y) / 6.f;
             v.z = (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z) / 6.f;
         } else {
-            v = velocity_at(g, u, p.x, p.y, p.z);
+            v = velocity_cached(g, u, p.x, p.y, p.z, c, cs, have);
         }
         p.x = clampf(p.x + dt * v.x, g.mn[0], g.mx[0]);
         p.y = clampf(p.y + dt * v.y, g.mn[1], g.mx[1]);

@@ -51,6 +51,9 @@ struct PlainDev {
     unsigned int *ticket;
     unsigned long long *step_ctr;
     float *u;            // [n_faces], signed
+    float2 *pairs;       // [3][V] per-voxel face pairs (x, y, z), signed
+    const int32_t *pair_dst;  // [n_active][2] float indices into pairs of each active face
+    int trace_blocks;    // persistent tracer grid: SMs x resident blocks per SM
     float4 *parts;       // [P] in cell (Morton) order
     const int32_t *perm; // [P] caller index of each stored particle
     GridDev grid;
@@ -73,6 +76,10 @@ int64_t n_faces_of(const psf_grid &g);
 // no voxel reads); PSF_ERR_SIGNS if two voxels read a face with different signs.
 int fold_signs(const psf_grid &g, const uint32_t *bits, std::vector<int8_t> &sigma);
 
+// For each active face, the two float slots of the per-voxel face-pair field
+// (float view of [3][V] float2) that hold its value: one in each adjacent voxel.
+void face_pair_slots(const psf_grid &g, const int32_t *faces, int64_t n_active, std::vector<int32_t> &dst);
+
 // Tracer constants of a grid (the reference's index offsets and box).
 GridDev make_grid_dev(const psf_grid &g);
 
@@ -83,6 +90,7 @@ int cuda_fail(cudaError_t e, const char *what);
 int launch_contract_state(const PlainDev &d, cudaStream_t st);
 int launch_reconstruct(const PlainDev &d, cudaStream_t st);
 int launch_trace(const PlainDev &d, cudaStream_t st);
+int trace_blocks_per_sm();
 int sort_particles_temp_bytes(long long P, size_t *bytes);
 int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);
 int launch_unorder_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);

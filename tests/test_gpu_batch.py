@@ -162,3 +162,39 @@ def test_batch_argument_errors(small_bases):
             batch.set_instance(0, 0, w0, L.make_params(), particles=np.zeros((300, 4), np.float32))
         with pytest.raises(L.PSFError):
             batch.get_state(0, 1)  # empty slot
+
+
+def test_step_limit_freezes_a_slot(small_bases):
+    """A slot with a step limit stops there while the others go on."""
+    b = small_bases["sphere12x10x9"]
+    spec_a, spec_b = SPECS[0], SPECS[3]
+    with Batch([b], slots=6, max_particles=1024) as batch:
+        w0, parts, f, params = _instance(b, spec_a)
+        batch.set_instance(0, spec_a[0], w0, params, particles=parts, forcing=f, steps=7)
+        _fill(batch, b, [spec_b])
+        batch.step(12)
+        assert batch.get_steps(0, spec_a[0]) == 7
+        assert batch.get_steps(0, spec_b[0]) == 12
+        ra, rb = _oracle(b, spec_a, 7), _oracle(b, spec_b, 12)
+        assert rel_err(batch.get_state(0, spec_a[0]), ra.w) <= W_TOL
+        assert np.abs(batch.get_particles(0, spec_a[0])[:, :3] - ra.pos).max() / b.h <= P_TOL_VOX
+        assert rel_err(batch.get_state(0, spec_b[0]), rb.w) <= W_TOL
+
+
+def test_particle_pool_admission(small_bases):
+    """Instances take ranges of a shared particle pool; a full pool refuses, a freed range is reused."""
+    b = small_bases["sphere12x10x9"]
+    with Batch([b], slots=6, max_particles=1024, particle_pool=1536) as batch:
+        assert batch.pool_free() == (1536, 1536)
+        _fill(batch, b, [SPECS[0], SPECS[3]])  # 300 -> 512 and 700 -> 768 particles
+        assert batch.pool_free()[0] == 1536 - 512 - 768
+        w0, parts, f, params = _instance(b, SPECS[1])  # 500 particles: no room
+        with pytest.raises(L.PSFError) as e:
+            batch.set_instance(0, SPECS[1][0], w0, params, particles=parts, forcing=f)
+        assert e.value.code == -3
+        batch.clear_instance(0, SPECS[0][0])
+        batch.set_instance(0, SPECS[1][0], w0, params, particles=parts, forcing=f)
+        batch.step(5)
+        ref = _oracle(b, SPECS[1], 5)
+        assert rel_err(batch.get_state(0, SPECS[1][0]), ref.w) <= W_TOL
+        assert np.abs(batch.get_particles(0, SPECS[1][0])[:, :3] - ref.pos).max() / b.h <= P_TOL_VOX
