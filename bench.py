@@ -72,6 +72,15 @@ BATCH_WORKLOADS = {
                  "64x32x32 channel in rotation, 16384 particles each, RK4"),
 }
 BIG_BASIS_CACHE = os.path.join(ROOT, ".basis_big")
+BASIS_CACHES = [os.path.join(ROOT, d) for d in (".basis_cache", ".basis_big", ".basis_c3")]
+
+
+def basis_cache_for(name, n):
+    """The cache directory holding a basis (full or compact file), else the large-basis cache."""
+    for d in BASIS_CACHES:
+        if any(os.path.exists(os.path.join(d, f"{name}_n{n}.{ext}")) for ext in ("psfb", "psfc")):
+            return d
+    return BIG_BASIS_CACHE
 DEFAULT_WORKLOAD = "sphere32_n128_p262144_rk4"
 FORM_WORKLOAD = "sphere32_n128_p262144_rk4_b64"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
@@ -175,7 +184,7 @@ def kernel_bytes(b, P, kind):
     if kind == "contract_state":
         return 4 * N * N * Np + 8 * N * 3
     if kind == "reconstruct":
-        return 4 * N * ((Fa + 3) // 4 * 4) + 4 * Fa + 4 * Fa + 8 * N
+        return 4 * Fa * Np + 4 * Fa + 4 * Fa + 8 * Fa + 8 * N
     return 32 * P  # trace: read + write float4 per particle
 
 
@@ -319,7 +328,7 @@ def run_ours(args, rank, world, local_rank):
     }
     line.update(extra)
     if rank == 0 and world == 1 and not args.no_forms:
-        form = run_batch(args, FORM_WORKLOAD, local_rank)
+        form = run_batch(args, FORM_WORKLOAD, local_rank, plain=False)
         form["speedup_vs_plain"] = round(form["value"] / value, 3)
         form["e2e_speedup_vs_plain"] = round(form["e2e"]["value"] / e2e["value"], 3)
         line["forms"] = {"batched_bf16x2": dict(workload=FORM_WORKLOAD, **form)}
@@ -392,9 +401,7 @@ def load_batch_workload(name, device):
     bases = []
     for spec, n in wl["bases"]:
         dom = make_domain(spec)
-        small = os.path.join(ROOT, ".basis_cache")
-        cache = small if os.path.exists(os.path.join(small, f"{dom.name}_n{n}.psfb")) else BIG_BASIS_CACHE
-        bases.append(cached_basis(dom, n, cache_dir=cache, device=device))
+        bases.append(cached_basis(dom, n, cache_dir=basis_cache_for(dom.name, n), device=device))
     rng = np.random.default_rng(4)
     insts = []
     for i in range(wl["instances"]):
@@ -443,7 +450,7 @@ def batch_kernel_bytes(bases, slots, insts, kind):
     return tot, flops
 
 
-def run_batch(args, name, local_rank, flush=True, check=True):
+def run_batch(args, name, local_rank, flush=True, check=True, plain=True):
     """Time a batched workload: device instance-steps/s, kernel roofline, e2e rollouts, FP64 error."""
     import torch
 
@@ -534,7 +541,44 @@ def run_batch(args, name, local_rank, flush=True, check=True):
     if check:
         out["accuracy"] = batch_accuracy(batch, wl, bases, insts, local_rank)
     batch.close()
+    if plain and args.plain_sample > 0:
+        out["plain_path"] = plain_sample(wl, bases, insts, local_rank, args.plain_sample)
+        out["speedup_vs_plain"] = round(value / out["plain_path"]["instance_steps_per_s"], 3)
     return out
+
+
+def plain_sample(wl, bases, insts, device, count):
+    """The plain FP32 single-instance path (one context per instance) on a sample of the same instances."""
+    import torch
+
+    from parallelspectralfluids3d_b200 import _lib as L
+    from parallelspectralfluids3d_b200.solver import Context
+
+    idx = np.linspace(0, len(insts) - 1, min(count, len(insts))).astype(int)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps, ms = 0, 0.0
+    for i in idx:
+        x = insts[i]
+        flags = L.PSF_FLAG_RENORM | (L.PSF_FLAG_FORCING if wl["force0"] else 0)
+        ctx = Context(bases[x["basis"]].truncate(x["n"]), L.make_params(dt=wl["dt"], integrator=wl["integrator"],
+                                                                         flags=flags), device=device)
+        if wl["force0"]:
+            ctx.set_forcing(x["force"])
+        ctx.set_state(x["w0"])
+        ctx.set_particles(x["parts"])
+        ctx.step(3)
+        ctx.sync()
+        st = torch.cuda.ExternalStream(ctx.stream)
+        k = 20
+        e0.record(st)
+        ctx.step(k)
+        e1.record(st)
+        ctx.sync()
+        ms += e0.elapsed_time(e1)
+        steps += k
+        ctx.close()
+    return {"instances": int(len(idx)), "steps_each": 20, "instance_steps_per_s": round(steps / (ms / 1e3), 1),
+            "note": "one context per instance, stepped back to back (graph replay), same inputs as the batch"}
 
 
 def batch_accuracy(batch, wl, bases, insts, device):
@@ -590,6 +634,9 @@ def run_batch_line(args, rank, world, local_rank):
             "clocks": clk, "batch": r["batch"]}
     if "accuracy" in r:
         line["accuracy"] = r["accuracy"]
+    for k in ("plain_path", "speedup_vs_plain"):
+        if k in r:
+            line[k] = r[k]
     return line
 
 
@@ -630,6 +677,144 @@ def run_reference_batch(args):
         "e2e": {"value": round(value, 3), "unit": "instance-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+
+
+# ------------------------------------------------------------ serving arm
+SERVE_WORKLOAD = "serve_poisson200"
+SERVE_DOMAINS = [(("box", 32, None), 256), (("sphere", 40, 10.0), 256), (("channel", (64, 32, 32), None), 256)]
+
+
+def serve_requests(seconds, rate=200.0, seed=7, n_max=256):
+    """Poisson request stream: arrival time, domain, N, steps, particle count, seeds."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            break
+        out.append(dict(t=t, basis=int(rng.integers(0, 3)), n=int(rng.integers(64, n_max + 1)),
+                        steps=int(rng.integers(50, 1001)), P=int(np.exp(rng.uniform(np.log(1e4), np.log(1e6)))),
+                        seed=int(rng.integers(0, 2**31 - 1))))
+    return out
+
+
+def run_serve(args, local_rank):
+    """Continuous-batching serving run: real-time Poisson arrivals through the engine."""
+    import threading
+
+    import torch
+
+    from parallelspectralfluids3d_b200 import _lib as L
+    from parallelspectralfluids3d_b200.engine import Engine
+    from parallelspectralfluids3d_b200.fixture import cached_basis, initial_coefficients, initial_particles
+
+    torch.cuda.set_device(local_rank)
+    bases = []
+    for spec, n in SERVE_DOMAINS:
+        dom = make_domain(spec)
+        bases.append(cached_basis(dom, n, cache_dir=basis_cache_for(dom.name, n), device="cuda"))
+    reqs = serve_requests(args.serve_seconds, n_max=min(b.n_modes for b in bases))
+    # Particle sources: one seeded cloud per domain, each request takes a slice.
+    clouds = [initial_particles(b, 2_000_000, 70 + i) for i, b in enumerate(bases)]
+    for q in reqs:
+        off = int(np.random.default_rng(q["seed"]).integers(0, 2_000_000 - q["P"]))
+        q["off"] = off
+        q["w0"] = initial_coefficients(q["n"], q["seed"])
+    params = L.make_params(dt=0.005, integrator=L.PSF_RK4, precision=L.PSF_PRECISION_BF16X2)
+    eng = Engine(bases, slots=args.serve_slots, max_particles=1_000_000, particle_pool=args.serve_pool,
+                 hbm_budget_bytes=int(args.serve_budget_gb * 2**30), chunk_steps=args.serve_chunk,
+                 device=local_rank, autotune=True)
+    ids = {}
+    lat, done = [], []
+    stop = threading.Event()
+
+    def producer():
+        t0 = time.perf_counter()
+        for i, q in enumerate(reqs):
+            dt = q["t"] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            parts = clouds[q["basis"]][q["off"]: q["off"] + q["P"]]
+            ids[eng.submit(q["basis"], q["w0"], q["steps"], params, particles=parts)] = i
+
+    def consumer():
+        while not stop.is_set() or len(done) < len(reqs):
+            got = eng.poll(4096)
+            if not got:
+                if stop.is_set() and len(done) >= len(reqs):
+                    break
+                time.sleep(0.002)
+                continue
+            for rid in got:
+                w, p, info = eng.collect(rid, want_particles=True)
+                lat.append(info["t_done"] - info["t_submit"])
+                done.append((ids.get(rid), info, w))
+
+    cons = threading.Thread(target=consumer)
+    cons.start()
+    t_start = time.perf_counter()
+    prod = threading.Thread(target=producer)
+    prod.start()
+    prod.join()
+    eng.drain(3600)
+    stop.set()
+    cons.join()
+    wall = time.perf_counter() - t_start
+    st = eng.stats()
+    eng.close()
+    lat = np.array(lat)
+    total_steps = sum(q["steps"] for q in reqs)
+    first = min(info["t_submit"] for _, info, _ in done)
+    last = max(info["t_done"] for _, info, _ in done)
+    out = {"requests": len(reqs), "completed": len(done), "arrival_window_s": args.serve_seconds,
+           "instance_steps": total_steps, "instance_steps_per_s": round(total_steps / (last - first), 1),
+           "particle_steps_per_s": round(st["particle_steps"] / (last - first), 1),
+           "p50_latency_s": round(float(np.percentile(lat, 50)), 4),
+           "p99_latency_s": round(float(np.percentile(lat, 99)), 4),
+           "mean_latency_s": round(float(lat.mean()), 4), "makespan_s": round(last - first, 3),
+           "wall_s": round(wall, 3), "engine": st,
+           "config": {"slots_per_domain": args.serve_slots, "particle_pool": args.serve_pool,
+                      "hbm_budget_gb": args.serve_budget_gb, "chunk_steps": args.serve_chunk,
+                      "n_range": [64, min(b.n_modes for b in bases)]}}
+    # Accuracy of a few served rollouts against the FP64 oracle (w only).
+    if not args.no_cpu:
+        from oracle import oracle as O
+
+        by_idx = {i: w for i, _, w in done if i is not None}
+        errs = []
+        for i in sorted(by_idx)[:3]:
+            q = reqs[i]
+            ref = O.OracleRollout(bases[q["basis"]].truncate(q["n"]), q["w0"], None, dt=0.005, integrator=4,
+                                  reconstruct=False).step(q["steps"])
+            errs.append({"request": i, "n_modes": q["n"], "steps": q["steps"],
+                         "rel_err_w_vs_fp64": float(np.linalg.norm(by_idx[i] - ref.w) / np.linalg.norm(ref.w))})
+        out["accuracy"] = errs
+    # The plain FP32 single-instance path on a sample of the same requests.
+    from parallelspectralfluids3d_b200.solver import Context
+
+    sample = reqs[: args.serve_plain_sample]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    plain_steps, plain_ms = 0, 0.0
+    for q in sample:
+        b = bases[q["basis"]].truncate(q["n"])
+        ctx = Context(b, L.make_params(dt=0.005, integrator=L.PSF_RK4), device=local_rank)
+        ctx.set_state(q["w0"])
+        ctx.set_particles(clouds[q["basis"]][q["off"]: q["off"] + q["P"]])
+        k = min(q["steps"], 50)
+        ctx.step(2)
+        ctx.sync()
+        st_ = torch.cuda.ExternalStream(ctx.stream)
+        ev0.record(st_)
+        ctx.step(k)
+        ev1.record(st_)
+        ctx.sync()
+        plain_ms += ev0.elapsed_time(ev1)
+        plain_steps += k
+        ctx.close()
+    out["plain_path_instance_steps_per_s"] = round(plain_steps / (plain_ms / 1e3), 1)
+    out["speedup_vs_plain"] = round(out["instance_steps_per_s"] / out["plain_path_instance_steps_per_s"], 3)
+    return out
+
 
 
 def run_for_profiler(args):
@@ -675,11 +860,19 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + [SERVE_WORKLOAD],
+                    default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the FP64 accuracy/CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched tensor-core form in the default line")
     ap.add_argument("--batch-steps", type=int, default=50, help="timed steps of a batched workload")
     ap.add_argument("--ncu-instances", type=int, default=0, help="profiling driver: only the first K instances")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving: length of the arrival window")
+    ap.add_argument("--serve-slots", type=int, default=96, help="serving: concurrent rollouts per domain")
+    ap.add_argument("--serve-pool", type=int, default=64_000_000, help="serving: particles resident at once")
+    ap.add_argument("--serve-budget-gb", type=float, default=16.0, help="serving: device budget of admitted rollouts")
+    ap.add_argument("--serve-chunk", type=int, default=8, help="serving: steps between admission rounds")
+    ap.add_argument("--serve-plain-sample", type=int, default=12, help="serving: requests timed on the plain path")
+    ap.add_argument("--plain-sample", type=int, default=12, help="batched: instances timed on the plain path")
     ap.add_argument("--ncu", type=int, default=0, metavar="S",
                     help="profiling driver: set up the workload, then run S steps kernel by kernel and exit")
     args = ap.parse_args()
@@ -705,6 +898,18 @@ def main():
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                               device_id=torch.device("cuda", local_rank))
+    if args.workload == SERVE_WORKLOAD:
+        if rank == 0:
+            clocks = ClockSampler(local_rank).start()
+            r = run_serve(args, local_rank)
+            clk = clocks.stop()
+            line = {"metric": "instance-steps/s", "value": r["instance_steps_per_s"], "unit": "instance-steps/s",
+                    "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "bf16x2", "state_dtype": "f64", "data": "synthetic",
+                    "p50_ms": round(1e3 * r["p50_latency_s"], 2), "p99_ms": round(1e3 * r["p99_latency_s"], 2),
+                    "config": {"workload": SERVE_WORKLOAD, **r.pop("config")}, "serve": r, "clocks": clk}
+            print(json.dumps(line), flush=True)
+        return
     try:
         if args.workload in BATCH_WORKLOADS:
             line = run_batch_line(args, rank, world, local_rank)

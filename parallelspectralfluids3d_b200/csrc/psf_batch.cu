@@ -79,6 +79,21 @@ __device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lan
     return v[0];
 }
 
+__device__ __forceinline__ float warp_reduce_scatter32f(float (&v)[32], int lane)
+{
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = (lane & s) != 0;
+#pragma unroll
+        for (int i = 0; i < s; ++i) {
+            const float send = upper ? v[i] : v[i + s];
+            const float keep = upper ? v[i + s] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+        }
+    }
+    return v[0];
+}
+
 template <int BN_MAX, int EPI>
 __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_constant__ GemmArgs args)
 {
@@ -212,28 +227,40 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
             int lt;
             const GemmGroup &G = args.g[find_group(args, t, &lt)];
             const int outer = lt / G.m_inner, inner = lt - outer * G.m_inner;
+            // Contraction: the state values of this warp's rows for the first
+            // 32 slots are loaded while the accumulator is still being computed.
+            float wv[32];
+            const int a_row = inner * 128 + row;
+            const bool arow = EPI == 0 && a_row < G.n_rows;
+            if (EPI == 0) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    wv[c] = (arow && c < G.cap) ? __ldg(G.wf + (size_t)c * G.ldw + a_row) : 0.f;
+            }
             bool ok = mbar_wait(&acc_full[abuf], aphase, err, ERR_WAIT_ACC_FULL);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             tc_fence_after();
             const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * BN_MAX);
             if (EPI == 0) {
-                // dw partial of mode k = outer over this warp's 32 rows a.
-                const int a = inner * 128 + row;
-                const bool arow = a < G.n_rows;
+                // dw partial of mode k = outer over this warp's 32 rows a:
+                // sum_a w[a][b] Y[a][b] for every slot b, in FP32.
                 for (int c0 = 0; c0 < G.bn; c0 += 32) {
                     float y[32];
                     tmem_ld32(tbase + (uint32_t)c0, y);
-                    double v[32];
 #pragma unroll
-                    for (int c = 0; c < 32; ++c) {
-                        const int b = c0 + c;
-                        v[c] = (arow && b < G.cap) ? (double)y[c] * __ldg(G.w + (size_t)b * G.ldw + a) : 0.0;
+                    for (int c = 0; c < 32; ++c) y[c] *= wv[c];
+                    if (c0 + 32 < G.bn) {
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            const int b = c0 + 32 + c;
+                            wv[c] = (arow && b < G.cap) ? __ldg(G.wf + (size_t)b * G.ldw + a_row) : 0.f;
+                        }
                     }
-                    const double s = warp_reduce_scatter32(v, lane);
+                    const float s = warp_reduce_scatter32f(y, lane);
                     const int b = c0 + lane;
                     if (b < G.cap)
-                        G.dwpart[((size_t)(outer * G.m_inner + inner) * 4 + q) * G.cap + b] = s;
+                        G.dwpart[((size_t)(outer * G.m_inner + inner) * 4 + q) * G.cap + b] = (double)s;
                 }
             } else {
                 // Face velocities of this warp's 32 rows, scattered into every
@@ -321,6 +348,7 @@ __global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restric
         v *= exp(s.visc_signed * G.lam[i] * s.dt);
         if (s.flags & PSF_FLAG_FORCING) v += s.dt * G.force[(size_t)b * G.N + i];
         w[i] = v;
+        G.wf[(size_t)b * G.N + i] = (float)v;
         split_bf16(v, Whi + i, Wlo + i);
     }
     if (threadIdx.x == 0) {
@@ -339,32 +367,67 @@ __global__ void psf_batch_pack(const GroupDev *__restrict__ groups, const SlotDe
     for (int i = threadIdx.x; i < G.Nj; i += blockDim.x) {
         const double v = (s.active && i < s.n_modes) ? G.w[(size_t)s.slot * G.N + i] : 0.0;
         split_bf16(v, Whi + i, Wlo + i);
+        if (i < G.N) G.wf[(size_t)s.slot * G.N + i] = (float)v;
     }
 }
 
 // ------------------------------------------------------------------ tracer
-__global__ void __launch_bounds__(256, 3) psf_batch_trace(const GroupDev *__restrict__ groups,
-                                                       const SlotDev *__restrict__ slots,
-                                                       const TraceItem *__restrict__ items,
-                                                       const int *__restrict__ n_items)
+// Every occupied slot's particles form one index space through the prefix
+// sums of the slots' particle counts; a particle finds its slot by binary
+// search in shared memory.  Slots that did not advance this step (step limit
+// reached) are skipped.
+__global__ void __launch_bounds__(128, 5) psf_batch_trace(const GroupDev *__restrict__ groups,
+                                                          const SlotDev *__restrict__ slots,
+                                                          const long long *__restrict__ prefix, int n_slots)
 {
-    const int n = *n_items;
-    for (int it = blockIdx.x; it < n; it += gridDim.x) {
-        const TraceItem ti = items[it];
-        if ((int)threadIdx.x >= ti.count) continue;
-        const SlotDev &s = slots[ti.slot_global];
-        if (!s.stepped) continue;
-        const GroupDev &G = groups[s.group];
-        const size_t idx = (size_t)s.poff + (size_t)ti.start + threadIdx.x;
-        TraceParams tp;
-        tp.dt = (float)s.dt;
-        tp.lifetime = s.lifetime;
-        tp.rk4 = s.rk4;
-        tp.seed = s.seed;
-        float4 p = G.parts[idx];
-        p = advance_particle(p, G.grid, G.pairs + (size_t)s.slot * 3 * (size_t)G.V, tp, s.step - 1ull,
-                             (uint32_t)G.perm[idx]);
-        G.parts[idx] = p;
+    __shared__ long long pre[BATCH_MAX_ALL_SLOTS + 1];
+    for (int i = threadIdx.x; i <= n_slots; i += blockDim.x) pre[i] = prefix[i];
+    __syncthreads();
+    const long long total = pre[n_slots];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // Parameters of the slot the thread is in, reloaded only when it changes.
+    int cur = -1;
+    bool live = false;
+    size_t base = 0;
+    TraceParams tp;
+    uint64_t step = 0;
+    const float2 *pairs = nullptr;
+    const GroupDev *G = nullptr;
+    for (long long gi = (long long)blockIdx.x * blockDim.x + threadIdx.x; gi < total; gi += stride) {
+        if (cur < 0 || gi >= pre[cur + 1]) {
+            int lo = cur < 0 ? 0 : cur;
+            int walk = 0;
+            while (pre[lo + 1] <= gi && walk < 8) {
+                ++lo;
+                ++walk;
+            }
+            if (pre[lo + 1] <= gi) {  // far away: binary search, pre[lo] <= gi < pre[hi]
+                int hi = n_slots;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (pre[mid] <= gi)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+            }
+            cur = lo;
+            const SlotDev &s = slots[cur];
+            live = s.stepped != 0;
+            G = groups + s.group;
+            base = (size_t)s.poff - (size_t)pre[cur];
+            tp.dt = (float)s.dt;
+            tp.lifetime = s.lifetime;
+            tp.rk4 = s.rk4;
+            tp.seed = s.seed;
+            step = s.step - 1ull;
+            pairs = G->pairs + (size_t)s.slot * 3 * (size_t)G->V;
+        }
+        if (!live) continue;
+        const size_t idx = base + (size_t)gi;
+        float4 p = G->parts[idx];
+        p = advance_particle(p, G->grid, pairs, tp, step, (uint32_t)G->perm[idx]);
+        G->parts[idx] = p;
     }
 }
 
@@ -440,15 +503,16 @@ int launch_batch_pack(const GroupDev *groups, const SlotDev *slots, int slot_glo
 int batch_trace_grid(int num_sms)
 {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_trace, 256, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_trace, 128, 0) != cudaSuccess || per_sm < 1)
         per_sm = 4;
     return num_sms * per_sm;
 }
 
-int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const TraceItem *items, const int *n_items,
-                       int grid, cudaStream_t st)
+int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const long long *prefix, int n_slots, int grid,
+                       cudaStream_t st)
 {
-    psf_batch_trace<<<grid, 256, 0, st>>>(groups, slots, items, n_items);
+    if (n_slots < 1 || n_slots > BATCH_MAX_ALL_SLOTS) return fail(PSF_ERR_INVALID, "slot count out of range");
+    psf_batch_trace<<<grid, 128, 0, st>>>(groups, slots, prefix, n_slots);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_batch_trace launch");
 }

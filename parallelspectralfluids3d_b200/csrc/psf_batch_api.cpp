@@ -4,7 +4,7 @@
 // TMA (K-major rows of 64 elements, 128-byte swizzle), the slots' FP64 state
 // and forcing, the BF16 hi/lo copy of the state used as the GEMMs' narrow
 // operand, the partial sums of the contraction, the slots' face fields and
-// particles; plus device tables of slots and tracer work items, so that one
+// particles; plus device tables of slots and of the slots' particle counts, so that one
 // captured CUDA graph serves every occupancy of the slots.
 
 #include <cuda_runtime.h>
@@ -49,6 +49,7 @@ struct HostGroup {
     uint16_t *Phi = nullptr;  // BF16 [2][Fp][Nj]
     uint16_t *W = nullptr;    // BF16 [2][bn][Nj]
     double *lam = nullptr, *w = nullptr, *force = nullptr, *dwpart = nullptr;
+    float *wf = nullptr;
     float2 *pairs = nullptr;
     std::vector<int32_t> faces_host, dst_host;  // for reading a slot's face field back
     int32_t *pair_dst = nullptr;
@@ -57,7 +58,7 @@ struct HostGroup {
 };
 
 // First-fit allocator of particle ranges in the batch's device pool, in
-// units of 256 particles (one tracer work item).
+// units of 256 particles.
 class RangePool {
 public:
     void reset(int64_t units)
@@ -127,13 +128,11 @@ struct psf_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<HostGroup> groups;
     std::vector<psf::SlotDev> slots;  // host mirror of the slot table
-    std::vector<psf::TraceItem> items;
+    std::vector<long long> prefix;  // host copy of the tracer's slot prefix sums
     psf::GroupDev *d_groups = nullptr;
     psf::SlotDev *d_slots = nullptr;
-    psf::TraceItem *d_items = nullptr;
-    int *d_n_items = nullptr;
+    long long *d_prefix = nullptr;
     int *d_err = nullptr;
-    int64_t item_cap = 0;
     psf::GemmArgs contract{};
     psf::GemmArgs recon{};
     int bn_max = 64;
@@ -218,6 +217,8 @@ int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
     const size_t cap = (size_t)G.cap;
     PSF_CHECK(B->alloc(&G.W, (size_t)2 * G.bn * G.Nj));
     PSF_CHECK(B->alloc(&G.w, cap * N));
+    PSF_CHECK(B->alloc(&G.wf, cap * N));
+    PSF_CUDA(cudaMemsetAsync(G.wf, 0, cap * N * 4, st));
     PSF_CHECK(B->alloc(&G.force, cap * N));
     PSF_CHECK(B->alloc(&G.dwpart, (size_t)N * G.a_tiles * 4 * cap));
     G.faces_host.assign(b.active_faces, b.active_faces + G.F_act);
@@ -276,7 +277,7 @@ void fill_gemm_args(psf_batch *B)
         x.cap = G.cap;
         x.n_rows = G.N;
         x.ldw = G.N;
-        x.w = G.w;
+        x.wf = G.wf;
         x.dwpart = G.dwpart;
         c.total_tiles += x.tiles;
         psf::GemmGroup &y = r.g[gi];
@@ -314,6 +315,7 @@ int upload_tables(psf_batch *B)
         d.n_faces = G.n_faces;
         d.pmax = G.pmax;
         d.w = G.w;
+        d.wf = G.wf;
         d.force = G.force;
         d.lam = G.lam;
         d.dwpart = G.dwpart;
@@ -331,21 +333,14 @@ int upload_tables(psf_batch *B)
     return PSF_OK;
 }
 
-int upload_items(psf_batch *B)
+int upload_prefix(psf_batch *B)
 {
-    B->items.clear();
-    for (const HostGroup &G : B->groups)
-        for (int b = 0; b < G.cap; ++b) {
-            const psf::SlotDev &s = B->slots[(size_t)(G.slot_base + b)];
-            if (!s.active) continue;
-            for (int64_t st = 0; st < s.n_particles; st += 256)
-                B->items.push_back({G.slot_base + b, (int)st, (int)std::min<int64_t>(256, s.n_particles - st), 0});
-        }
-    const int n = (int)B->items.size();
-    if (n > 0)
-        PSF_CUDA(cudaMemcpyAsync(B->d_items, B->items.data(), (size_t)n * sizeof(psf::TraceItem),
-                                 cudaMemcpyHostToDevice, B->stream));
-    PSF_CUDA(cudaMemcpyAsync(B->d_n_items, &n, sizeof(int), cudaMemcpyHostToDevice, B->stream));
+    const size_t n = B->slots.size();
+    B->prefix.assign(n + 1, 0);
+    for (size_t s = 0; s < n; ++s)
+        B->prefix[s + 1] = B->prefix[s] + (B->slots[s].active ? B->slots[s].n_particles : 0);
+    PSF_CUDA(cudaMemcpyAsync(B->d_prefix, B->prefix.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice,
+                             B->stream));
     PSF_CUDA(cudaStreamSynchronize(B->stream));
     return PSF_OK;
 }
@@ -415,7 +410,7 @@ int launch_step(psf_batch *B, cudaStream_t st)
     PSF_CHECK(psf::launch_batch_gemm(B->contract, 0, B->bn_max, B->gemm_ctas, st));
     PSF_CHECK(psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st));
     PSF_CHECK(psf::launch_batch_gemm(B->recon, 1, B->bn_max, B->gemm_ctas, st));
-    PSF_CHECK(psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_items, B->d_n_items, B->trace_ctas, st));
+    PSF_CHECK(psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_prefix, B->n_slots(), B->trace_ctas, st));
     return PSF_OK;
 }
 
@@ -559,11 +554,10 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
         if (B->pool_cap > (int64_t)INT32_MAX) return bail(fail(PSF_ERR_UNSUPPORTED, "particle pool too large"));
         B->pool.reset(B->pool_cap / 256);
         B->slot_units.assign((size_t)slot_base, 0);
-        B->item_cap = B->pool_cap / 256 + slot_base;
     }
     if ((rc = B->alloc(&B->pool_parts, (size_t)B->pool_cap)) || (rc = B->alloc(&B->pool_perm, (size_t)B->pool_cap)) ||
         (rc = B->alloc(&B->d_groups, B->groups.size())) || (rc = B->alloc(&B->d_slots, B->slots.size())) ||
-        (rc = B->alloc(&B->d_items, (size_t)B->item_cap)) || (rc = B->alloc(&B->d_n_items, 1)))
+        (rc = B->alloc(&B->d_prefix, B->slots.size() + 1)))
         return bail(rc);
     // Particle ordering scratch, sized for the largest slot.
     {
@@ -577,7 +571,7 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
         o.temp = temp;
         o.temp_bytes = tmp;
     }
-    if ((rc = upload_tables(B)) != PSF_OK || (rc = upload_items(B)) != PSF_OK) return bail(rc);
+    if ((rc = upload_tables(B)) != PSF_OK || (rc = upload_prefix(B)) != PSF_OK) return bail(rc);
     fill_gemm_args(B);
     B->trace_ctas = psf::batch_trace_grid(B->num_sms);
     B->gemm_ctas = cfg->gemm_ctas > 0 ? cfg->gemm_ctas : B->num_sms;
@@ -648,7 +642,7 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
         s.active = 0;
         s.n_particles = 0;
         PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, st));
-        PSF_CHECK(upload_items(B));
+        PSF_CHECK(upload_prefix(B));
         return fail(PSF_ERR_NOMEM, "the particle pool has no free range for this instance");
     }
     B->slot_units[(size_t)sg] = units;
@@ -677,7 +671,7 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
                                  cudaMemcpyHostToDevice, st));
         PSF_CHECK(psf::launch_order_particles(particle_view(B, basis, slot, inst->n_particles), B->order, st));
     }
-    PSF_CHECK(upload_items(B));
+    PSF_CHECK(upload_prefix(B));
     PSF_CUDA(cudaStreamSynchronize(st));
     return PSF_OK;
 }
@@ -700,7 +694,7 @@ int psf_batch_clear_instance(psf_batch *B, int32_t basis, int32_t slot)
     PSF_CUDA(cudaMemsetAsync(G.w + (size_t)slot * G.N, 0, (size_t)G.N * 8, B->stream));
     PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, B->stream));
     PSF_CHECK(psf::launch_batch_pack(B->d_groups, B->d_slots, sg, B->stream));
-    PSF_CHECK(upload_items(B));
+    PSF_CHECK(upload_prefix(B));
     return PSF_OK;
 }
 
@@ -825,7 +819,7 @@ int psf_batch_profile_step(psf_batch *B, double *kernel_ms, int32_t n)
     if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, B->bn_max, B->gemm_ctas, st);
     cudaEventRecord(ev[3], st);
     if (rc == PSF_OK)
-        rc = psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_items, B->d_n_items, B->trace_ctas, st);
+        rc = psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_prefix, B->n_slots(), B->trace_ctas, st);
     cudaEventRecord(ev[4], st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");

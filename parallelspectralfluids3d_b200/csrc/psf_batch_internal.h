@@ -13,6 +13,7 @@ namespace psf {
 
 constexpr int BATCH_MAX_GROUPS = 6;   // distinct bases in one batch
 constexpr int BATCH_MAX_SLOTS = 256;  // instance slots per basis (one MMA N tile)
+constexpr int BATCH_MAX_ALL_SLOTS = BATCH_MAX_GROUPS * BATCH_MAX_SLOTS;
 constexpr int GEMM_THREADS = 192;     // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 
 // One basis inside a GEMM launch: A operand (C or Phi) and B operand (the
@@ -29,7 +30,7 @@ struct alignas(64) GemmGroup {
     int cap;                // slots in use (columns)
     int n_rows;             // valid rows: N (contraction) or F_act (reconstruction)
     int ldw;                // row stride of w (= the basis' N)
-    const double *w;        // contraction: FP64 state [cap][ldw]
+    const float *wf;        // contraction: FP32 copy of the state [cap][ldw]
     double *dwpart;         // contraction: partials [((k*m_inner + at)*4 + q)][cap]
     long long n_faces;
     const int32_t *pair_dst;  // reconstruction: [n_rows][2] float slots in a slot's face pairs
@@ -71,6 +72,7 @@ struct GroupDev {
     int N, Nj, cap, bn, a_tiles, slot_base;
     long long n_faces, pmax;
     double *w;            // [cap][N]
+    float *wf;            // [cap][N] FP32 copy of w (contraction epilogue)
     double *force;        // [cap][N]
     const double *lam;    // [N]
     double *dwpart;       // see GemmGroup
@@ -81,21 +83,15 @@ struct GroupDev {
     int32_t *perm;        // caller index of each pooled particle
 };
 
-// One tracer work item: up to 256 particles of one slot.
-struct TraceItem {
-    int slot_global;
-    int start;
-    int count;
-    int pad;
-};
 
 // Launchers (psf_batch.cu).  `bn_max` selects the kernel variant (64, 128 or
 // 256 MMA columns per accumulator); `grid` the number of persistent CTAs.
 int batch_gemm_smem_bytes(int bn_max);
 int launch_batch_gemm(const GemmArgs &args, int epilogue, int bn_max, int grid, cudaStream_t st);
 int launch_batch_state(const GroupDev *groups, SlotDev *slots, int n_slots, cudaStream_t st);
-int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const TraceItem *items, const int *n_items,
-                       int grid, cudaStream_t st);
+// prefix[s] = particles of slots 0..s-1 (occupied slots only); n_slots + 1 entries.
+int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const long long *prefix, int n_slots, int grid,
+                       cudaStream_t st);
 int launch_batch_pack(const GroupDev *groups, const SlotDev *slots, int slot_global, cudaStream_t st);
 int batch_trace_grid(int num_sms);
 

@@ -14,7 +14,8 @@ namespace psf {
 
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
-__device__ __forceinline__ float mixf(float x, float y, float a) { return x * (1.f - a) + y * a; }
+// glm::mix(x, y, a) = x (1 - a) + y a, evaluated as x + a (y - x) (one FMA).
+__device__ __forceinline__ float mixf(float x, float y, float a) { return fmaf(a, y - x, x); }
 
 // Counter-based generator for respawns (SplitMix64 output function); the
 // oracle uses the same function so respawns are reproducible.
@@ -80,10 +81,10 @@ __device__ __forceinline__ Cell cell_of(const GridDev &g, float px, float py, fl
     gw.y = (py - g.mn[1]) * g.inv_h;
     gw.z = (pz - g.mn[2]) * g.inv_h;
     Cell c;
-    c.xO = clampi((int)floorf(gix), 0, g.nx - 1);
-    c.yO = clampi((int)floorf(giy), 0, g.ny - 1);
-    c.zO = clampi((int)floorf(giz), 0, g.nz - 1);
-    const int xr = (int)floorf(gix - 0.5f), yr = (int)floorf(giy - 0.5f), zr = (int)floorf(giz - 0.5f);
+    c.xO = clampi(__float2int_rd(gix), 0, g.nx - 1);
+    c.yO = clampi(__float2int_rd(giy), 0, g.ny - 1);
+    c.zO = clampi(__float2int_rd(giz), 0, g.nz - 1);
+    const int xr = __float2int_rd(gix - 0.5f), yr = __float2int_rd(giy - 0.5f), zr = __float2int_rd(giz - 0.5f);
     c.xM = clampi(xr, 0, g.nx - 1);
     c.xP = clampi(xr + 1, 0, g.nx - 1);
     c.yM = clampi(yr, 0, g.ny - 1);

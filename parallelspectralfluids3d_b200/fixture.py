@@ -15,6 +15,11 @@ Solver/abstractsolver.h:111-126):
 File format ``.psfb`` (little endian): a 256-byte header followed by the
 arrays in header order; see :data:`HEADER` and ``include/psf/basis_file.h``.
 Any prefix ``N' <= N`` of a basis is again a basis (:meth:`Basis.truncate`).
+
+Compact files ``.psfc`` (header version 2) store Phi as FP32 and leave C out;
+loading one promotes Phi to FP64 and rebuilds C from it with the same tensor
+builder (FP64 GEMMs, on the GPU when there is one).  The loaded arrays are the
+basis: the device path and the oracle consume exactly the same Phi and C.
 """
 
 from __future__ import annotations
@@ -29,6 +34,7 @@ from .domain import Domain
 
 MAGIC = b"PSFBASIS"
 VERSION = 1
+COMPACT_VERSION = 2
 # magic, version, dims[3], h, aabb_min[3], aabb_max[3], n_modes, n_faces,
 # n_active, n_voxels, n_sign_words, then 7 array offsets (bytes from file start).
 HEADER = struct.Struct("<8sI3Id3f3fiqqqq7Q")
@@ -91,13 +97,14 @@ class Basis:
         return full
 
     # ------------------------------------------------------------- file io
-    def save(self, path: str) -> None:
+    def save(self, path: str, compact: bool = False) -> None:
+        """Write a ``.psfb`` file, or with ``compact`` a ``.psfc`` (Phi FP32, no C)."""
         arrays = [
             np.ascontiguousarray(self.active_faces, dtype="<i4"),
             np.ascontiguousarray(self.lam, dtype="<f8"),
             np.ascontiguousarray(self.gravity, dtype="<f8"),
-            np.ascontiguousarray(self.phi, dtype="<f8"),
-            np.ascontiguousarray(self.C, dtype="<f8"),
+            np.ascontiguousarray(self.phi, dtype="<f4" if compact else "<f8"),
+            np.zeros(0, dtype="<f8") if compact else np.ascontiguousarray(self.C, dtype="<f8"),
             np.ascontiguousarray(self.sign_bits, dtype="<u4"),
             np.ascontiguousarray(self.inside, dtype="u1"),
         ]
@@ -107,7 +114,7 @@ class Basis:
             offsets.append(pos)
             pos += a.nbytes
         hdr = HEADER.pack(
-            MAGIC, VERSION, *[int(d) for d in self.dims], float(self.h),
+            MAGIC, COMPACT_VERSION if compact else VERSION, *[int(d) for d in self.dims], float(self.h),
             *[float(v) for v in self.aabb_min], *[float(v) for v in self.aabb_max],
             self.n_modes, self.n_faces, self.n_active, self.n_voxels, int(self.sign_bits.size),
             *offsets,
@@ -121,12 +128,13 @@ class Basis:
         os.replace(tmp, path)
 
     @staticmethod
-    def load(path: str, name: str | None = None) -> "Basis":
+    def load(path: str, name: str | None = None, device: str | None = None) -> "Basis":
         with open(path, "rb") as f:
             raw = f.read()
         vals = HEADER.unpack_from(raw, 0)
-        if vals[0] != MAGIC or vals[1] != VERSION:
-            raise ValueError(f"{path}: not a version-{VERSION} basis file")
+        if vals[0] != MAGIC or vals[1] not in (VERSION, COMPACT_VERSION):
+            raise ValueError(f"{path}: not a basis file")
+        compact = vals[1] == COMPACT_VERSION
         dims = tuple(vals[2:5])
         h = vals[5]
         amin = np.array(vals[6:9], dtype=np.float32)
@@ -138,13 +146,17 @@ class Basis:
             a = np.frombuffer(raw, dtype=dtype, count=count, offset=off[i]).copy()
             return a.reshape(shape) if shape else a
 
-        return Basis(
+        phi = arr(3, "<f4", Fa * N, (Fa, N)).astype(np.float64) if compact else arr(3, "<f8", Fa * N, (Fa, N))
+        b = Basis(
             dims, h, amin, amax,
             arr(0, "<i4", Fa), arr(1, "<f8", N), arr(2, "<f8", N),
-            arr(3, "<f8", Fa * N, (Fa, N)), arr(4, "<f8", N * N * N, (N, N, N)),
+            phi, None if compact else arr(4, "<f8", N * N * N, (N, N, N)),
             arr(5, "<u4", nw), arr(6, "u1", V),
             name=name or os.path.splitext(os.path.basename(path))[0],
         )
+        if compact:
+            b.C = rebuild_tensor(b, device)
+        return b
 
 
 def build_basis(dom: Domain, n_modes: int, device: str = "cpu") -> Basis:
@@ -165,6 +177,24 @@ def build_basis(dom: Domain, n_modes: int, device: str = "cpu") -> Basis:
     )
 
 
+def rebuild_tensor(b: Basis, device: str | None = None) -> np.ndarray:
+    """C of a basis from its Phi and eigenvalues (the tensor builder of :func:`build_basis`)."""
+    from . import basis as B
+
+    if device is None:
+        try:
+            import torch
+
+            device = "cuda" if torch.cuda.is_available() else "cpu"
+        except Exception:
+            device = "cpu"
+    dom = b.domain()
+    dom.build()
+    phi_full = b.phi_full()
+    psi = B.curl_basis(dom, phi_full)
+    return B.advection_tensor(dom, phi_full, psi, b.lam, device=device)
+
+
 def cached_basis(dom: Domain, n_modes: int, cache_dir: str | None = None,
                  device: str = "cpu") -> Basis:
     """Build a basis once and keep it as ``<cache_dir>/<domain>_n<N>.psfb``."""
@@ -175,6 +205,9 @@ def cached_basis(dom: Domain, n_modes: int, cache_dir: str | None = None,
     path = os.path.join(cache_dir, f"{dom.name}_n{n_modes}.psfb")
     if os.path.exists(path):
         return Basis.load(path, name=dom.name)
+    compact = os.path.join(cache_dir, f"{dom.name}_n{n_modes}.psfc")
+    if os.path.exists(compact):
+        return Basis.load(compact, name=dom.name, device=None if device == "cpu" else device)
     b = build_basis(dom, n_modes, device=device)
     b.save(path)
     return b

@@ -79,3 +79,20 @@ def test_gravity_projection(small_bases):
     m = dom.face_inside & (ny_ != 0)
     g[m] = np.where(ny_[m] > 0, 1.0, -1.0) * 0.00981
     assert np.allclose(b.gravity, phi.T @ g)
+
+
+def test_compact_basis_file_round_trip(tmp_path, small_bases):
+    """A .psfc keeps Phi as FP32 and rebuilds C from it on load."""
+    from parallelspectralfluids3d_b200.fixture import Basis
+
+    b = small_bases["sphere12x10x9"]
+    path = str(tmp_path / "b.psfc")
+    b.save(path, compact=True)
+    c = Basis.load(path, device="cpu")
+    assert np.array_equal(c.phi, b.phi.astype(np.float32).astype(np.float64))
+    assert np.array_equal(c.lam, b.lam) and np.array_equal(c.active_faces, b.active_faces)
+    assert np.abs(c.C - b.C).max() <= 1e-5 * np.abs(b.C).max()
+    # C of the loaded basis is the tensor of its own Phi: rebuilding again gives the same array.
+    from parallelspectralfluids3d_b200.fixture import rebuild_tensor
+
+    assert np.array_equal(rebuild_tensor(c, "cpu"), c.C)
