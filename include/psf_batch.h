@@ -46,6 +46,10 @@ typedef struct psf_batch_config {
     int32_t gemm_ctas;               /* 0 (one per SM), or force the persistent grid size */
     int64_t particle_pool;           /* particles resident at once over all slots (device pool);
                                         0 = every slot at its max_particles */
+    int32_t contraction_ksplit;      /* 0 (1, or the autotuner's choice), or force 1, 2 or 4 K ranges
+                                        per contraction row tile */
+    int32_t unfused;                 /* 0: one cooperative tensor-core launch per step (contraction,
+                                        state update, reconstruction); 1: three launches */
 } psf_batch_config;
 
 /* One instance placed in a slot. */
@@ -69,6 +73,7 @@ typedef struct psf_batch_info {
     int32_t kernels_per_step;  /* launches per psf_batch_step(b, 1) */
     int64_t device_bytes;      /* device memory held by the batch */
     double tuned_ms;           /* GEMM time of the chosen variant at tuning (0 if not tuned) */
+    int32_t contraction_ksplit; /* K ranges per contraction row tile (1, 2 or 4) */
 } psf_batch_info;
 
 int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out);
@@ -98,9 +103,13 @@ int psf_batch_get_particles(psf_batch *b, int32_t basis, int32_t slot, float *xy
 int psf_batch_get_velocity(psf_batch *b, int32_t basis, int32_t slot, float *u, int64_t n_faces);
 int psf_batch_get_steps(psf_batch *b, int32_t basis, int32_t slot, int64_t *steps);
 
-/* One step with each kernel timed between CUDA events (milliseconds, launch
- * order: contraction GEMM, state update, reconstruction GEMM, tracer). */
+/* One step, run as psf_batch_step runs it, with each launch timed between
+ * CUDA events (milliseconds): [tensor-core step, tracer] for a fused batch,
+ * [contraction, state update, reconstruction, tracer] otherwise. */
 int psf_batch_profile_step(psf_batch *b, double *kernel_ms, int32_t n);
+/* One step as three tensor-core launches plus the tracer, each timed
+ * (milliseconds): [contraction, state update, reconstruction, tracer]. */
+int psf_batch_profile_phases(psf_batch *b, double *kernel_ms, int32_t n);
 
 /* Device error word of the tensor-core kernels: 0, or the code of a bounded
  * wait that gave up (the batch must then be destroyed). */

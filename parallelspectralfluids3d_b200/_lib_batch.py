@@ -13,7 +13,7 @@ BATCH_EXPORTS = (
     "psf_batch_create", "psf_batch_destroy", "psf_batch_info_get", "psf_batch_set_instance",
     "psf_batch_clear_instance", "psf_batch_step", "psf_batch_sync", "psf_batch_get_stream",
     "psf_batch_get_state", "psf_batch_get_particles", "psf_batch_get_velocity", "psf_batch_get_steps",
-    "psf_batch_profile_step", "psf_batch_device_status", "psf_batch_pool_free",
+    "psf_batch_profile_step", "psf_batch_profile_phases", "psf_batch_device_status", "psf_batch_pool_free",
 )
 
 
@@ -34,6 +34,8 @@ class BatchConfig(ct.Structure):
         ("gemm_columns", ct.c_int32),
         ("gemm_ctas", ct.c_int32),
         ("particle_pool", ct.c_int64),
+        ("contraction_ksplit", ct.c_int32),
+        ("unfused", ct.c_int32),
     ]
 
 
@@ -57,6 +59,7 @@ class BatchInfo(ct.Structure):
         ("kernels_per_step", ct.c_int32),
         ("device_bytes", ct.c_int64),
         ("tuned_ms", ct.c_double),
+        ("contraction_ksplit", ct.c_int32),
     ]
 
 
@@ -77,5 +80,6 @@ def declare(lib) -> None:
     lib.psf_batch_get_velocity.argtypes = [vp, i32, i32, vp, ct.c_int64]
     lib.psf_batch_get_steps.argtypes = [vp, i32, i32, ct.POINTER(ct.c_int64)]
     lib.psf_batch_profile_step.argtypes = [vp, ct.POINTER(ct.c_double), i32]
+    lib.psf_batch_profile_phases.argtypes = [vp, ct.POINTER(ct.c_double), i32]
     lib.psf_batch_device_status.argtypes = [vp, ct.POINTER(i32)]
     lib.psf_batch_pool_free.argtypes = [vp, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]

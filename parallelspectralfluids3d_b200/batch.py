@@ -21,7 +21,8 @@ class Batch:
     """Slots of one or more bases stepped together (BF16 hi/lo tensor-core path)."""
 
     def __init__(self, bases, slots, max_particles, device: int = 0, autotune: bool = True,
-                 gemm_columns: int = 0, gemm_ctas: int = 0, particle_pool: int = 0):
+                 gemm_columns: int = 0, gemm_ctas: int = 0, particle_pool: int = 0, ksplit: int = 0,
+                 fused: bool = True):
         """``bases``: list of :class:`~.fixture.Basis`; ``slots`` / ``max_particles``: per basis (int or list)."""
         self.lib = L.load()
         n = len(bases)
@@ -45,6 +46,8 @@ class Batch:
         cfg.gemm_columns = int(gemm_columns)
         cfg.gemm_ctas = int(gemm_ctas)
         cfg.particle_pool = int(particle_pool)
+        cfg.contraction_ksplit = int(ksplit)
+        cfg.unfused = 0 if fused else 1
         self.handle = ct.c_void_p()
         L.check(self.lib.psf_batch_create(ct.byref(cfg), int(device), ct.byref(self.handle)))
         self._n_modes = {}
@@ -114,8 +117,16 @@ class Batch:
         return int(s.value or 0)
 
     def profile_step(self) -> np.ndarray:
+        """Device ms of each launch of one step: [tensor-core step, tracer] when fused."""
+        n = self.info()["kernels_per_step"]
+        out = np.zeros(n, dtype=np.float64)
+        L.check(self.lib.psf_batch_profile_step(self.handle, out.ctypes.data_as(ct.POINTER(ct.c_double)), n))
+        return out
+
+    def profile_phases(self) -> np.ndarray:
+        """Device ms of [contraction, state update, reconstruction, tracer] run as separate launches."""
         out = np.zeros(4, dtype=np.float64)
-        L.check(self.lib.psf_batch_profile_step(self.handle, out.ctypes.data_as(ct.POINTER(ct.c_double)), 4))
+        L.check(self.lib.psf_batch_profile_phases(self.handle, out.ctypes.data_as(ct.POINTER(ct.c_double)), 4))
         return out
 
     def info(self) -> dict:

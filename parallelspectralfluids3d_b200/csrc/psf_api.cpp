@@ -300,6 +300,7 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     d.Np = (int)round_up(N, 4);
     d.S = std::max(1, std::min(N, (2 * c->num_sms + N - 1) / N));
     d.n_active = b->n_active;
+    d.ldp = round_up(b->n_active, 4);
     d.n_faces = F;
     d.P = 0;
 
@@ -309,15 +310,15 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         for (int64_t ka = 0; ka < (int64_t)N * N; ++ka)
             for (int j = 0; j < N; ++j) hC[(size_t)ka * d.Np + j] = (float)b->advection[(size_t)ka * N + j];
         // Phi mode-major with the tracer's face signs folded in.
-        std::vector<float> hP((size_t)b->n_active * d.Np, 0.f);
+        std::vector<float> hP((size_t)N * d.ldp, 0.f);
         for (int64_t r = 0; r < b->n_active; ++r) {
             const float s = (float)c->sigma[(size_t)b->active_faces[r]];
-            for (int i = 0; i < N; ++i) hP[(size_t)r * d.Np + i] = s * (float)b->phi[(size_t)r * N + i];
+            for (int i = 0; i < N; ++i) hP[(size_t)i * d.ldp + r] = s * (float)b->phi[(size_t)r * N + i];
         }
-        float *C = nullptr, *phi = nullptr;
+        float *C = nullptr, *phiT = nullptr;
         int32_t *faces = nullptr;
         double *lam = nullptr, *force = nullptr;
-        if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phi, hP.size())) ||
+        if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phiT, hP.size())) ||
             (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&d.w, (size_t)N)) ||
             (rc = c->alloc(&d.dwpart, (size_t)N * d.S)) || (rc = c->alloc(&lam, (size_t)N)) ||
             (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
@@ -334,13 +335,13 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
             (e = cudaStreamSynchronize(c->stream)))
             return bail(psf::cuda_fail(e, "face pair upload"));
         d.C = C;
-        d.phi = phi;
+        d.phiT = phiT;
         d.faces = faces;
         d.lam = lam;
         d.force = force;
         cudaStream_t st = c->stream;
         if ((e = cudaMemcpyAsync(C, hC.data(), hC.size() * 4, cudaMemcpyHostToDevice, st)) ||
-            (e = cudaMemcpyAsync(phi, hP.data(), hP.size() * 4, cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(phiT, hP.data(), hP.size() * 4, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(faces, b->active_faces, (size_t)b->n_active * 4, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(lam, b->eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemsetAsync(force, 0, (size_t)N * 8, st)) || (e = cudaMemsetAsync(d.w, 0, (size_t)N * 8, st)) ||

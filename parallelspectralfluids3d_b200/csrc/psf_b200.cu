@@ -9,9 +9,10 @@
 //      finish (atomic ticket, no spinning) applies the FP64 state update:
 //      Euler step, energy renormalisation, viscous decay, forcing.
 //      (replaces simulation.cl:207-311 and :356-394, five OpenCL kernels)
-//   2. psf_reconstruct     u = Phi w with Phi stored face-major (the tracer's
-//      face signs folded in), so a block streams a contiguous stretch of Phi;
-//      scatter to the reference face numbering and to the per-voxel face pairs.
+//   2. psf_reconstruct     u = Phi w with Phi stored mode-major (faces
+//      contiguous, the tracer's face signs folded in), so every warp streams
+//      512 contiguous bytes per mode; scatter to the reference face numbering
+//      and to the per-voxel face pairs.
 //      (replaces simulation.cl:313-354)
 //   3. psf_trace           one thread per particle, trilinear staggered
 //      interpolation from the signed face field, RK1 or RK4, box clamp,
@@ -139,62 +140,55 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
 }
 
 // ---------------------------------------------------- 2. reconstruction
-// Phi is stored face-major, so a warp streams whole faces: lane l holds
-// w[4l + 128c .. +3] in registers and loads the matching float4 of each face;
-// one warp reduction per face.  A block of 8 warps covers 8 x RECON_FPW
-// consecutive faces, i.e. one contiguous stretch of Phi.
-template <int CH>
-__host__ __device__ constexpr int recon_fpw()
-{
-    return CH <= 2 ? 8 : (CH <= 4 ? 4 : 2);
-}
-
-template <int CH>
-__global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__ phi, int Np,
+// 256 threads = 8 warps x 32 lanes; a block covers 128 consecutive active
+// faces (4 per lane, one float4 per mode); warp g sums modes i = g (mod 8).
+__global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__ phiT, long long ldp,
                                                        const int32_t *__restrict__ faces, long long n_active,
                                                        int N, const double *__restrict__ w, float *__restrict__ u,
                                                        float *__restrict__ pairs,
                                                        const int32_t *__restrict__ pair_dst)
 {
-    constexpr int RECON_FPW = recon_fpw<CH>();
+    __shared__ float wsm[PSF_MAX_MODES];
+    __shared__ float4 red[8][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float wr[CH][4];
+    for (int i = threadIdx.x; i < N; i += 256) wsm[i] = (float)w[i];
+    __syncthreads();
+    const long long f0 = (long long)blockIdx.x * 128 + lane * 4;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (f0 < ldp) {
+        const float *base = phiT + f0;
+#pragma unroll 8
+        for (int i = warp; i < N; i += 8) {
+            const float4 v = __ldcs(reinterpret_cast<const float4 *>(base + (size_t)i * ldp));
+            const float wi = wsm[i];
+            acc.x = fmaf(v.x, wi, acc.x);
+            acc.y = fmaf(v.y, wi, acc.y);
+            acc.z = fmaf(v.z, wi, acc.z);
+            acc.w = fmaf(v.w, wi, acc.w);
+        }
+    }
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        float4 t = red[0][lane];
 #pragma unroll
-    for (int c = 0; c < CH; ++c)
+        for (int g = 1; g < 8; ++g) {
+            const float4 r = red[g][lane];
+            t.x += r.x;
+            t.y += r.y;
+            t.z += r.z;
+            t.w += r.w;
+        }
+        const float vals[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int col = c * 128 + lane * 4 + q;
-            wr[c][q] = col < N ? (float)w[col] : 0.f;
-        }
-    const long long f0 = ((long long)blockIdx.x * 8 + warp) * RECON_FPW;
-    float4 v[RECON_FPW][CH];
-#pragma unroll
-    for (int t = 0; t < RECON_FPW; ++t)
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const long long f = f0 + t;
-            v[t][c] = (f < n_active && c * 128 + lane * 4 < Np)
-                          ? __ldcs(reinterpret_cast<const float4 *>(phi + (size_t)f * Np) + c * 32 + lane)
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-#pragma unroll
-    for (int t = 0; t < RECON_FPW; ++t) {
-        float s = 0.f;
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            s = fmaf(v[t][c].x, wr[c][0], s);
-            s = fmaf(v[t][c].y, wr[c][1], s);
-            s = fmaf(v[t][c].z, wr[c][2], s);
-            s = fmaf(v[t][c].w, wr[c][3], s);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        const long long f = f0 + t;
-        if (lane == 0 && f < n_active) {
-            u[faces[f]] = s;
-            const int32_t d0 = pair_dst[2 * f], d1 = pair_dst[2 * f + 1];
-            if (d0 >= 0) pairs[d0] = s;
-            if (d1 >= 0) pairs[d1] = s;
+            const long long r = f0 + q;
+            if (r < n_active) {
+                u[faces[r]] = vals[q];
+                const int32_t d0 = pair_dst[2 * r], d1 = pair_dst[2 * r + 1];
+                if (d0 >= 0) pairs[d0] = vals[q];
+                if (d1 >= 0) pairs[d1] = vals[q];
+            }
         }
     }
 }
@@ -303,26 +297,9 @@ int launch_contract_state(const PlainDev &d, cudaStream_t st)
 
 int launch_reconstruct(const PlainDev &d, cudaStream_t st)
 {
-    const int CH = (d.Np + 127) / 128;
-    float *pf = reinterpret_cast<float *>(d.pairs);
-#define PSF_CASE(n)                                                                                    \
-    case n:                                                                                            \
-        psf_reconstruct<n><<<(unsigned)((d.n_active + 8 * recon_fpw<n>() - 1) / (8 * recon_fpw<n>())), 256, 0, st>>>(d.phi, d.Np, d.faces, d.n_active, d.N, d.w, d.u, pf, \
-                                                   d.pair_dst);                                        \
-        break;
-    switch (CH) {
-        PSF_CASE(1)
-        PSF_CASE(2)
-        PSF_CASE(3)
-        PSF_CASE(4)
-        PSF_CASE(5)
-        PSF_CASE(6)
-        PSF_CASE(7)
-        PSF_CASE(8)
-    default:
-        return fail(PSF_ERR_UNSUPPORTED, "mode count above the supported maximum");
-    }
-#undef PSF_CASE
+    const long long blocks = (d.n_active + 127) / 128;
+    psf_reconstruct<<<(unsigned)blocks, 256, 0, st>>>(d.phiT, d.ldp, d.faces, d.n_active, d.N, d.w, d.u,
+                                                      reinterpret_cast<float *>(d.pairs), d.pair_dst);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_reconstruct launch");
 }

@@ -14,14 +14,17 @@
 // fewer modes than the basis are zero-padded, which is exact: their W rows
 // beyond N_b are zero, and dw_k for k >= N_b is ignored.
 //
-// psf_batch_gemm is one persistent kernel per GEMM over the tiles of every
-// basis: warp 0 streams 128-row A tiles and the W tile through a TMA ring of
+// psf_batch_step_tc is one persistent kernel over the tiles of every basis:
+// warp 0 streams 128-row A tiles and the W tile through a TMA ring of
 // shared-memory stages (128-byte swizzle, no multicast), warp 1 issues the
 // tcgen05.mma chain for a tile into one of two TMEM accumulators, warps 2-5
 // drain the other accumulator (tcgen05.ld) and run the epilogue, so loads,
-// MMAs and epilogue overlap.  The FP64 state update of every slot
-// (psf_batch_state) and the tracer (psf_batch_trace, the same interpolant as
-// the single-instance path) complete the step.
+// MMAs and epilogue overlap.  In the default (fused) step one cooperative
+// launch runs the contraction, the FP64 state update of every slot and the
+// reconstruction, separated by bounded grid barriers; the tracer
+// (psf_batch_trace, the same interpolant as the single-instance path)
+// completes the step.  Unfused launches (one GEMM each, plus
+// psf_batch_state) serve autotuning and per-phase profiling.
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -52,33 +55,40 @@ struct GemmCfg {
     static constexpr int SMEM = STAGES * STAGE_BYTES + BAR_BYTES + 1024;  // + alignment slack
 };
 
-__device__ __forceinline__ int find_group(const GemmArgs &args, int t, int *local)
+// Work unit t of a launch: contraction units first, then reconstruction units.
+__device__ __forceinline__ const GemmGroup &unit_group(const StepArgs &a, int t, bool &recon, int *local)
 {
+    recon = t >= a.c_tiles;
+    int base = recon ? a.n_groups : 0;
+    int u = recon ? t - a.c_tiles : t;
     int g = 0;
-    while (g + 1 < args.n_groups && t >= args.g[g].tiles) {
-        t -= args.g[g].tiles;
+    while (g + 1 < a.n_groups && u >= a.g[base + g].tiles) {
+        u -= a.g[base + g].tiles;
         ++g;
     }
-    *local = t;
-    return g;
+    *local = u;
+    return a.g[base + g];
+}
+
+// Work unit -> (outer index, row tile, K range [kc0, kc1)).
+struct Unit {
+    int outer, inner, ks, kc0, kc1;
+};
+
+__device__ __forceinline__ Unit decode_unit(const GemmGroup &G, int lt)
+{
+    Unit u;
+    const int per_outer = G.m_inner * G.ksplit;
+    u.outer = lt / per_outer;
+    const int rem = lt - u.outer * per_outer;
+    u.inner = rem / G.ksplit;
+    u.ks = rem - u.inner * G.ksplit;
+    u.kc0 = u.ks * G.kc_per;
+    u.kc1 = min(G.k_chunks, u.kc0 + G.kc_per);
+    return u;
 }
 
 // 32 values per lane -> lane l holds the sum over the warp of value l.
-__device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lane)
-{
-#pragma unroll
-    for (int s = 16; s >= 1; s >>= 1) {
-        const bool upper = (lane & s) != 0;
-#pragma unroll
-        for (int i = 0; i < s; ++i) {
-            const double send = upper ? v[i] : v[i + s];
-            const double keep = upper ? v[i + s] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
-        }
-    }
-    return v[0];
-}
-
 __device__ __forceinline__ float warp_reduce_scatter32f(float (&v)[32], int lane)
 {
 #pragma unroll
@@ -94,8 +104,110 @@ __device__ __forceinline__ float warp_reduce_scatter32f(float (&v)[32], int lane
     return v[0];
 }
 
-template <int BN_MAX, int EPI>
-__global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_constant__ GemmArgs args)
+__device__ __forceinline__ double warp_allsum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Grid-wide barrier of a cooperative launch: arrive, then wait (bounded) until
+// `target` arrivals were counted.  Called by one thread per CTA after a CTA
+// barrier, as the cooperative-groups grid sync does.
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, unsigned int target, int *err)
+{
+    __threadfence();
+    atomicAdd(bar, 1u);
+    const unsigned long long t0 = globaltimer();
+    for (;;) {
+        unsigned int v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+        if (v >= target) break;
+        if (globaltimer() - t0 > PSF_WAIT_LIMIT_NS) {
+            record_error(err, ERR_GRID_SYNC);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    __threadfence();
+    return true;
+}
+
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *hi, __nv_bfloat16 *lo)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    *hi = h;
+    *lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+}
+
+// FP64 update of one slot by the 128 epilogue threads of a CTA, in the
+// reference's order (psfsolver.cpp:37-59), then the new state's FP32 copy and
+// BF16 hi/lo split.  Energy sums: per warp (shuffles), then the 4 warps in
+// fixed order, so the result does not depend on timing.
+__device__ void state_update_cta(const GroupDev *__restrict__ groups, SlotDev &s, int et, double *red)
+{
+    const int lane = et & 31, ew = et >> 5;
+    if (!s.active) return;  // uniform over the 128 threads
+    if (s.target != 0ull && s.step >= s.target) {
+        if (et == 0) s.stepped = 0;
+        return;
+    }
+    const GroupDev &G = groups[s.group];
+    const int b = s.slot, N = s.n_modes, parts = G.nparts;
+    double *w = G.w + (size_t)b * G.N;
+    double e1 = 0.0, e2 = 0.0;
+    for (int i = et; i < N; i += 128) {
+        double dw = 0.0;
+        const double *dp = G.dwpart + ((size_t)b * G.N + i) * parts;
+        for (int p = 0; p < parts; ++p) dw += dp[p];
+        const double wi = w[i];
+        const double w1 = wi + s.dt * dw;
+        w[i] = w1;
+        e1 += wi * wi;
+        e2 += w1 * w1;
+    }
+    e1 = warp_allsum(e1);
+    e2 = warp_allsum(e2);
+    if (lane == 0) {
+        red[ew] = e1;
+        red[4 + ew] = e2;
+    }
+    epilogue_bar();
+    e1 = red[0] + red[1] + red[2] + red[3];
+    e2 = red[4] + red[5] + red[6] + red[7];
+    const double scale = (s.flags & PSF_FLAG_RENORM) ? sqrt(e1 / e2) : 1.0;
+    __nv_bfloat16 *Whi = reinterpret_cast<__nv_bfloat16 *>(G.W) + (size_t)b * G.Nj;
+    __nv_bfloat16 *Wlo = Whi + (size_t)G.bn * G.Nj;
+    for (int i = et; i < N; i += 128) {
+        double v = w[i] * scale;
+        v *= exp(s.visc_signed * G.lam[i] * s.dt);
+        if (s.flags & PSF_FLAG_FORCING) v += s.dt * G.force[(size_t)b * G.N + i];
+        w[i] = v;
+        G.wf[(size_t)b * G.N + i] = (float)v;
+        split_bf16(v, Whi + i, Wlo + i);
+    }
+    epilogue_bar();  // red[] is reused by the next slot
+    if (et == 0) {
+        s.step += 1ull;
+        s.stepped = 1;
+    }
+}
+
+// One launch of the tensor-core step.  Warp 0: TMA producer; warp 1: MMA
+// issuer; warps 2-5: TMEM epilogue.  Unfused launches run their contraction
+// or reconstruction units.  A fused launch (cooperative) is one whole step of
+// the coefficient pipeline: the epilogue warps first update every slot's
+// state from the contraction partials of the previous launch (FP64, one CTA
+// per slot), a grid barrier makes the new coefficients visible, and then
+// one sweep runs the reconstruction of the new state together with the
+// contraction that the next step's update will use (both need only the new
+// coefficients).  During the update the producer already loads the first
+// tiles of C and Phi, which do not depend on the state, and issues their
+// coefficient (W) loads once the barrier has passed.
+template <int BN_MAX>
+__global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __grid_constant__ StepArgs args)
 {
     using Cfg = GemmCfg<BN_MAX>;
     constexpr int STAGES = Cfg::STAGES;
@@ -107,10 +219,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
     uint64_t *empty = bars + STAGES;
     uint64_t *acc_full = bars + 2 * STAGES;
     uint64_t *acc_empty = acc_full + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2);
+    uint64_t *wready = acc_empty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(wready + 1);
+    double *red = reinterpret_cast<double *>(wready + 2);  // 8 doubles (bytes 8*(2*STAGES+6) .. +64)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int *err = args.err;
+    const int total = args.c_tiles + args.r_tiles;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -121,8 +236,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
             mbar_init(&acc_full[b], 1);
             mbar_init(&acc_empty[b], 128);
         }
+        mbar_init(wready, 1);
         mbar_fence_init();
-        for (int g = 0; g < args.n_groups; ++g) {
+        for (int g = 0; g < 2 * args.n_groups; ++g) {
             tma_prefetch_desc(&args.g[g].tmA);
             tma_prefetch_desc(&args.g[g].tmB);
         }
@@ -141,12 +257,30 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
             uint32_t last_parity[STAGES];
             bool issued[STAGES];
             for (int s = 0; s < STAGES; ++s) issued[s] = false;
+            // Reconstruction stages whose W load waits for the state update.
+            int pend_stage[STAGES], pend_kc[STAGES], pend_t[STAGES];
+            int npend = 0;
+            bool w_ok = !args.fused;
             bool ok = true;
-            for (int t = blockIdx.x; ok && t < args.total_tiles; t += gridDim.x) {
+            auto flush = [&]() -> bool {
+                if (!mbar_wait(wready, 0u, err, ERR_WAIT_STATE)) return false;
+                for (int i = 0; i < npend; ++i) {
+                    bool rc;
+                    int lt;
+                    const GemmGroup &G = unit_group(args, pend_t[i], rc, &lt);
+                    unsigned char *sB = smem + pend_stage[i] * Cfg::STAGE_BYTES + Cfg::A_BYTES;
+                    tma_load_3d(sB, &G.tmB, &full[pend_stage[i]], pend_kc[i] * 64, 0, 0);
+                }
+                npend = 0;
+                w_ok = true;
+                return true;
+            };
+            for (int t = blockIdx.x; ok && t < total; t += gridDim.x) {
+                bool recon;
                 int lt;
-                const GemmGroup &G = args.g[find_group(args, t, &lt)];
-                const int outer = lt / G.m_inner, inner = lt - outer * G.m_inner;
-                for (int kc = 0; kc < G.k_chunks; ++kc) {
+                const GemmGroup &G = unit_group(args, t, recon, &lt);
+                const Unit un = decode_unit(G, lt);
+                for (int kc = un.kc0; kc < un.kc1; ++kc) {
                     if (!mbar_wait(&empty[stage], phase ^ 1u, err, ERR_WAIT_EMPTY)) {
                         ok = false;
                         break;
@@ -154,18 +288,30 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
                     unsigned char *sA = smem + stage * Cfg::STAGE_BYTES;
                     unsigned char *sB = sA + Cfg::A_BYTES;
                     mbar_arrive_expect_tx(&full[stage], G.tx_bytes);
-                    tma_load_4d(sA, &G.tmA, &full[stage], kc * 64, inner * 128, 0, outer);
-                    tma_load_3d(sB, &G.tmB, &full[stage], kc * 64, 0, 0);
+                    tma_load_4d(sA, &G.tmA, &full[stage], kc * 64, un.inner * 128, 0, un.outer);
+                    if (!w_ok) {
+                        pend_stage[npend] = stage;
+                        pend_kc[npend] = kc;
+                        pend_t[npend] = t;
+                        ++npend;
+                    } else {
+                        tma_load_3d(sB, &G.tmB, &full[stage], kc * 64, 0, 0);
+                    }
                     issued[stage] = true;
                     last_parity[stage] = phase;
                     if (++stage == STAGES) {
                         stage = 0;
                         phase ^= 1u;
                     }
+                    if (npend == STAGES && !flush()) {
+                        ok = false;
+                        break;
+                    }
                 }
             }
-            // After an error elsewhere, copies may still be in flight that no
-            // one consumes: wait (bounded) for them before the CTA exits.
+            if (ok && npend > 0) ok = flush();
+            // After an error, copies may still be in flight that no one
+            // consumes: wait (bounded) for them before the CTA exits.
             if (*(volatile int *)err != 0)
                 for (int s = 0; s < STAGES; ++s)
                     if (issued[s]) mbar_wait(&full[s], last_parity[s], err, ERR_WAIT_DRAIN);
@@ -178,14 +324,16 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
             int abuf = 0;
             uint32_t aphase = 0;
             bool ok = true;
-            for (int t = blockIdx.x; ok && t < args.total_tiles; t += gridDim.x) {
+            for (int t = blockIdx.x; ok && t < total; t += gridDim.x) {
+                bool recon;
                 int lt;
-                const GemmGroup &G = args.g[find_group(args, t, &lt)];
+                const GemmGroup &G = unit_group(args, t, recon, &lt);
+                const Unit un = decode_unit(G, lt);
                 if (!mbar_wait(&acc_empty[abuf], aphase ^ 1u, err, ERR_WAIT_ACC_EMPTY)) break;
                 tc_fence_after();
                 const uint32_t d = tmem_base + (uint32_t)(abuf * BN_MAX);
                 const uint32_t idesc = idesc_bf16_f32(128, G.bn);
-                for (int kc = 0; kc < G.k_chunks; ++kc) {
+                for (int kc = un.kc0; kc < un.kc1; ++kc) {
                     if (!mbar_wait(&full[stage], phase, err, ERR_WAIT_FULL)) {
                         ok = false;
                         break;
@@ -199,7 +347,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
                         const uint64_t al = desc_kmajor_sw128(a0 + 128 * 128 + kk * 32);
                         const uint64_t bh = desc_kmajor_sw128(b0 + kk * 32);
                         const uint64_t bl = desc_kmajor_sw128(b0 + (uint32_t)G.bn * 128u + kk * 32);
-                        mma_bf16(d, ah, bh, idesc, (kc | kk) ? 1u : 0u);
+                        mma_bf16(d, ah, bh, idesc, (kc != un.kc0 || kk != 0) ? 1u : 0u);
                         mma_bf16(d, ah, bl, idesc, 1u);
                         mma_bf16(d, al, bh, idesc, 1u);
                     }
@@ -219,30 +367,46 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
         }
     } else {
         // -------------------------------------------------------- epilogue
-        const int q = warp & 3;  // TMEM lanes 32q .. 32q+31 belong to this warp
+        const int q = warp & 3;   // TMEM lanes 32q .. 32q+31 belong to this warp
         const int row = q * 32 + lane;
         int abuf = 0;
         uint32_t aphase = 0;
-        for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
+        if (args.fused) {
+            // Every slot's state update (one CTA per slot), then a grid
+            // barrier before any coefficient (W) load of the sweep.
+            const int et = threadIdx.x - 64;
+            for (int s = blockIdx.x; s < args.n_slots; s += gridDim.x)
+                state_update_cta(args.groups, args.slots[s], et, red);
+            // The new coefficients are read next by TMA (the async proxy).
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            epilogue_bar();
+            if (threadIdx.x == 64) {
+                if (grid_sync(args.grid_bar, gridDim.x, err)) mbar_arrive(wready);
+            }
+            epilogue_bar();  // the epilogue reads other CTAs' new state (wf) below
+        }
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            bool recon;
             int lt;
-            const GemmGroup &G = args.g[find_group(args, t, &lt)];
-            const int outer = lt / G.m_inner, inner = lt - outer * G.m_inner;
+            const GemmGroup &G = unit_group(args, t, recon, &lt);
+            const Unit un = decode_unit(G, lt);
+            const int outer = un.outer, inner = un.inner;
             // Contraction: the state values of this warp's rows for the first
             // 32 slots are loaded while the accumulator is still being computed.
             float wv[32];
             const int a_row = inner * 128 + row;
-            const bool arow = EPI == 0 && a_row < G.n_rows;
-            if (EPI == 0) {
+            const bool arow = !recon && a_row < G.n_rows;
+            if (!recon) {
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
-                    wv[c] = (arow && c < G.cap) ? __ldg(G.wf + (size_t)c * G.ldw + a_row) : 0.f;
+                    wv[c] = (arow && c < G.cap) ? __ldcg(G.wf + (size_t)c * G.ldw + a_row) : 0.f;
             }
             bool ok = mbar_wait(&acc_full[abuf], aphase, err, ERR_WAIT_ACC_FULL);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             tc_fence_after();
             const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(abuf * BN_MAX);
-            if (EPI == 0) {
+            if (!recon) {
                 // dw partial of mode k = outer over this warp's 32 rows a:
                 // sum_a w[a][b] Y[a][b] for every slot b, in FP32.
                 for (int c0 = 0; c0 < G.bn; c0 += 32) {
@@ -254,13 +418,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
 #pragma unroll
                         for (int c = 0; c < 32; ++c) {
                             const int b = c0 + 32 + c;
-                            wv[c] = (arow && b < G.cap) ? __ldg(G.wf + (size_t)b * G.ldw + a_row) : 0.f;
+                            wv[c] = (arow && b < G.cap) ? __ldcg(G.wf + (size_t)b * G.ldw + a_row) : 0.f;
                         }
                     }
                     const float s = warp_reduce_scatter32f(y, lane);
                     const int b = c0 + lane;
                     if (b < G.cap)
-                        G.dwpart[((size_t)(outer * G.m_inner + inner) * 4 + q) * G.cap + b] = (double)s;
+                        G.dwpart[((size_t)b * G.n_rows + outer) * G.nparts + (inner * G.ksplit + un.ks) * 4 + q] =
+                            (double)s;
                 }
             } else {
                 // Face velocities of this warp's 32 rows, scattered into every
@@ -303,13 +468,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_gemm(const __grid_c
 }
 
 // ------------------------------------------------------------ state update
-__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *hi, __nv_bfloat16 *lo)
-{
-    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
-    *hi = h;
-    *lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
-}
-
 // FP64 update of one slot in the reference's order (psfsolver.cpp:37-59),
 // then the new state's BF16 hi/lo split for the next products.
 __global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restrict__ groups,
@@ -324,14 +482,13 @@ __global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restric
         return;
     }
     const GroupDev &G = groups[s.group];
-    const int b = s.slot, N = s.n_modes, at = G.a_tiles, cap = G.cap;
+    const int b = s.slot, N = s.n_modes, parts = G.nparts;
     double *w = G.w + (size_t)b * G.N;
     double e1 = 0.0, e2 = 0.0;
     for (int i = threadIdx.x; i < N; i += 256) {
         double dw = 0.0;
-        for (int t = 0; t < at; ++t)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) dw += G.dwpart[((size_t)(i * at + t) * 4 + q) * cap + b];
+        const double *dp = G.dwpart + ((size_t)b * G.N + i) * parts;
+        for (int p = 0; p < parts; ++p) dw += dp[p];
         const double wi = w[i];
         const double w1 = wi + s.dt * dw;
         wnew[i] = w1;
@@ -442,8 +599,8 @@ int batch_gemm_smem_bytes(int bn_max)
     }
 }
 
-template <int BN, int EPI>
-static int launch_gemm_t(const GemmArgs &args, int grid, cudaStream_t st)
+template <int BN>
+static int launch_tc_t(const StepArgs &args, int grid, cudaStream_t st)
 {
     // The shared-memory limit is a per-device attribute of the kernel.
     static unsigned long long configured = 0;
@@ -452,37 +609,71 @@ static int launch_gemm_t(const GemmArgs &args, int grid, cudaStream_t st)
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(configured & bit)) {
-        e = cudaFuncSetAttribute(psf_batch_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(psf_batch_step_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  GemmCfg<BN>::SMEM);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(psf_batch_gemm)");
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(psf_batch_step_tc)");
         configured |= bit;
     }
-    psf_batch_gemm<BN, EPI><<<grid, GEMM_THREADS, GemmCfg<BN>::SMEM, st>>>(args);
-    e = cudaGetLastError();
-    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_batch_gemm launch");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(GEMM_THREADS);
+    cfg.dynamicSmemBytes = GemmCfg<BN>::SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = args.fused ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, psf_batch_step_tc<BN>, args);
+    if (e != cudaSuccess) return cuda_fail(e, "psf_batch_step_tc launch");
+    return PSF_OK;
 }
 
-int launch_batch_gemm(const GemmArgs &args, int epilogue, int bn_max, int grid, cudaStream_t st)
+int launch_batch_step_tc(const StepArgs &args, int bn_max, int grid, cudaStream_t st)
 {
-    if (args.total_tiles <= 0) return PSF_OK;
-    grid = std::max(1, std::min(grid, args.total_tiles));
-    for (int g = 0; g < args.n_groups; ++g)
-        if (args.g[g].bn > bn_max || args.g[g].bn % 16 != 0 || args.g[g].bn < 16)
+    const int total = args.c_tiles + args.r_tiles;
+    if (total <= 0 && !args.fused) return PSF_OK;
+    if (!args.fused) grid = std::min(grid, total);
+    grid = std::max(1, grid);
+    for (int g = 0; g < 2 * args.n_groups; ++g) {
+        const bool used = g < args.n_groups ? args.c_tiles > 0 : args.r_tiles > 0;
+        if (used && (args.g[g].bn > bn_max || args.g[g].bn % 16 != 0 || args.g[g].bn < 16))
             return fail(PSF_ERR_INVALID, "GEMM group N tile does not fit the kernel variant");
-    if (epilogue == 0) {
-        switch (bn_max) {
-        case 64: return launch_gemm_t<64, 0>(args, grid, st);
-        case 128: return launch_gemm_t<128, 0>(args, grid, st);
-        case 256: return launch_gemm_t<256, 0>(args, grid, st);
-        }
-    } else {
-        switch (bn_max) {
-        case 64: return launch_gemm_t<64, 1>(args, grid, st);
-        case 128: return launch_gemm_t<128, 1>(args, grid, st);
-        case 256: return launch_gemm_t<256, 1>(args, grid, st);
-        }
+    }
+    switch (bn_max) {
+    case 64: return launch_tc_t<64>(args, grid, st);
+    case 128: return launch_tc_t<128>(args, grid, st);
+    case 256: return launch_tc_t<256>(args, grid, st);
     }
     return fail(PSF_ERR_UNSUPPORTED, "GEMM variant must have 64, 128 or 256 columns");
+}
+
+// Largest persistent grid a cooperative launch of the variant can hold.
+int max_fused_grid(int bn_max, int num_sms)
+{
+    int per_sm = 0;
+    cudaError_t e = cudaSuccess;
+    switch (bn_max) {
+    case 64:
+        cudaFuncSetAttribute(psf_batch_step_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<64>::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<64>, GEMM_THREADS,
+                                                          GemmCfg<64>::SMEM);
+        break;
+    case 128:
+        cudaFuncSetAttribute(psf_batch_step_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GemmCfg<128>::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<128>, GEMM_THREADS,
+                                                          GemmCfg<128>::SMEM);
+        break;
+    default:
+        cudaFuncSetAttribute(psf_batch_step_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GemmCfg<256>::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<256>, GEMM_THREADS,
+                                                          GemmCfg<256>::SMEM);
+        break;
+    }
+    if (e != cudaSuccess) return 0;
+    return per_sm * num_sms;
 }
 
 int launch_batch_state(const GroupDev *groups, SlotDev *slots, int n_slots, cudaStream_t st)

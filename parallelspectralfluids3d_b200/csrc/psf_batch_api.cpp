@@ -42,6 +42,7 @@ inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 struct HostGroup {
     int N = 0, Nj = 0, Na = 0, a_tiles = 0;
     int cap = 0, bn = 0, slot_base = 0;
+    int parts = 4;  // contraction partials per mode (a-tiles x K splits x 4 warps)
     int64_t F_act = 0, Fp = 0, n_faces = 0, pmax = 0;
     psf_grid grid{};
     std::vector<int8_t> sigma;
@@ -133,9 +134,13 @@ struct psf_batch {
     psf::SlotDev *d_slots = nullptr;
     long long *d_prefix = nullptr;
     int *d_err = nullptr;
-    psf::GemmArgs contract{};
-    psf::GemmArgs recon{};
+    psf::StepArgs contract{};   // contraction units only
+    psf::StepArgs recon{};      // reconstruction units only
+    psf::StepArgs fused{};      // contraction, state update, reconstruction in one cooperative launch
+    bool use_fused = true;
+    unsigned int *grid_bar = nullptr;
     int bn_max = 64;
+    int ksplit = 1;   // K ranges per contraction row tile
     int gemm_ctas = 148;
     int trace_ctas = 592;
     double tuned_ms = 0.0;
@@ -220,7 +225,7 @@ int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
     PSF_CHECK(B->alloc(&G.wf, cap * N));
     PSF_CUDA(cudaMemsetAsync(G.wf, 0, cap * N * 4, st));
     PSF_CHECK(B->alloc(&G.force, cap * N));
-    PSF_CHECK(B->alloc(&G.dwpart, (size_t)N * G.a_tiles * 4 * cap));
+    PSF_CHECK(B->alloc(&G.dwpart, (size_t)N * G.a_tiles * 4 * psf::GEMM_MAX_KSPLIT * cap));
     G.faces_host.assign(b.active_faces, b.active_faces + G.F_act);
     psf::face_pair_slots(G.grid, b.active_faces, G.F_act, G.dst_host);
     PSF_CHECK(B->alloc(&G.pair_dst, G.dst_host.size()));
@@ -231,7 +236,7 @@ int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
     PSF_CUDA(cudaMemsetAsync(G.W, 0, (size_t)2 * G.bn * G.Nj * 2, st));
     PSF_CUDA(cudaMemsetAsync(G.w, 0, cap * N * 8, st));
     PSF_CUDA(cudaMemsetAsync(G.force, 0, cap * N * 8, st));
-    PSF_CUDA(cudaMemsetAsync(G.dwpart, 0, (size_t)N * G.a_tiles * 4 * cap * 8, st));
+    PSF_CUDA(cudaMemsetAsync(G.dwpart, 0, (size_t)N * G.a_tiles * 4 * psf::GEMM_MAX_KSPLIT * cap * 8, st));
 
     // Tensor maps: inner dimension first, strides in bytes for dims 1..
     {
@@ -257,21 +262,30 @@ int upload_basis(psf_batch *B, HostGroup &G, const psf_batch_basis &bb)
 
 void fill_gemm_args(psf_batch *B)
 {
-    psf::GemmArgs &c = B->contract;
-    psf::GemmArgs &r = B->recon;
+    psf::StepArgs &c = B->contract;
+    psf::StepArgs &r = B->recon;
     std::memset(&c, 0, sizeof(c));
-    std::memset(&r, 0, sizeof(r));
-    c.n_groups = r.n_groups = (int)B->groups.size();
-    c.err = r.err = B->d_err;
-    for (size_t gi = 0; gi < B->groups.size(); ++gi) {
-        HostGroup &G = B->groups[gi];
+    const int n = (int)B->groups.size();
+    c.n_groups = n;
+    c.err = B->d_err;
+    c.grid_bar = B->grid_bar;
+    c.groups = B->d_groups;
+    c.slots = B->d_slots;
+    c.n_slots = B->n_slots();
+    for (int gi = 0; gi < n; ++gi) {
+        HostGroup &G = B->groups[(size_t)gi];
         const uint32_t tx = 2u * 128u * 128u + 2u * (uint32_t)G.bn * 128u;
         psf::GemmGroup &x = c.g[gi];
         x.tmA = G.mapC;
         x.tmB = G.mapW;
         x.m_inner = G.a_tiles;
-        x.tiles = G.N * G.a_tiles;
         x.k_chunks = G.Nj / 64;
+        x.ksplit = std::max(1, std::min(B->ksplit, x.k_chunks));
+        x.kc_per = (x.k_chunks + x.ksplit - 1) / x.ksplit;
+        x.ksplit = (x.k_chunks + x.kc_per - 1) / x.kc_per;  // no empty K range
+        x.tiles = G.N * G.a_tiles * x.ksplit;
+        G.parts = G.a_tiles * x.ksplit * 4;
+        x.nparts = G.parts;
         x.bn = G.bn;
         x.tx_bytes = tx;
         x.cap = G.cap;
@@ -279,13 +293,15 @@ void fill_gemm_args(psf_batch *B)
         x.ldw = G.N;
         x.wf = G.wf;
         x.dwpart = G.dwpart;
-        c.total_tiles += x.tiles;
-        psf::GemmGroup &y = r.g[gi];
+        c.c_tiles += x.tiles;
+        psf::GemmGroup &y = c.g[n + gi];
         y.tmA = G.mapPhi;
         y.tmB = G.mapW;
         y.tiles = (int)(G.Fp / 128);
         y.m_inner = y.tiles;
         y.k_chunks = G.Nj / 64;
+        y.ksplit = 1;
+        y.kc_per = y.k_chunks;
         y.bn = G.bn;
         y.tx_bytes = tx;
         y.cap = G.cap;
@@ -295,8 +311,13 @@ void fill_gemm_args(psf_batch *B)
         y.pair_dst = G.pair_dst;
         y.pairs = reinterpret_cast<float *>(G.pairs);
         y.pair_floats = 6 * G.V;
-        r.total_tiles += y.tiles;
+        c.r_tiles += y.tiles;
     }
+    B->fused = c;
+    B->fused.fused = 1;
+    r = c;
+    r.c_tiles = 0;     // reconstruction units only
+    c.r_tiles = 0;     // contraction units only
 }
 
 int upload_tables(psf_batch *B)
@@ -311,6 +332,7 @@ int upload_tables(psf_batch *B)
         d.cap = G.cap;
         d.bn = G.bn;
         d.a_tiles = G.a_tiles;
+        d.nparts = G.parts;
         d.slot_base = G.slot_base;
         d.n_faces = G.n_faces;
         d.pmax = G.pmax;
@@ -355,44 +377,70 @@ int check_device_error(psf_batch *B)
     return PSF_OK;
 }
 
+int fused_grid(psf_batch *B)
+{
+    return std::max(1, std::min(B->gemm_ctas, psf::max_fused_grid(B->bn_max, B->num_sms)));
+}
+
+// The tensor-core part of a step: one cooperative launch (fused), or the
+// contraction, the state kernel and the reconstruction as three launches.
+int launch_tc_part(psf_batch *B, cudaStream_t st, bool fused)
+{
+    if (fused) {
+        PSF_CUDA(cudaMemsetAsync(B->grid_bar, 0, sizeof(unsigned int), st));
+        return psf::launch_batch_step_tc(B->fused, B->bn_max, fused_grid(B), st);
+    }
+    PSF_CHECK(psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, st));
+    PSF_CHECK(psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st));
+    PSF_CHECK(psf::launch_batch_step_tc(B->recon, B->bn_max, B->gemm_ctas, st));
+    return PSF_OK;
+}
+
 // Project-written autotuner: time every kernel variant that fits the batch
-// (MMA columns 64 / 128 / 256, i.e. 4 / 3 / 2 pipeline stages, and persistent
-// grids of 1x and 1/2x the SM count) on both GEMMs and keep the fastest.
+// (MMA columns 64 / 128 / 256, i.e. 4 / 3 / 2 pipeline stages; persistent
+// grids of 1x and 1/2x the SM count; 1, 2 or 4 K ranges per contraction row
+// tile) on the tensor-core part of a step exactly as the step will run it
+// (one fused launch, or three launches), and keep the fastest.  Run at
+// creation, when every slot is empty, so the timed launches change nothing.
 int autotune(psf_batch *B, int need_bn)
 {
     const int variants[3] = {64, 128, 256};
     const int grids[2] = {B->num_sms, std::max(1, B->num_sms / 2)};
+    const int splits[3] = {1, 2, 4};
     cudaEvent_t e0, e1;
     PSF_CUDA(cudaEventCreate(&e0));
     PSF_CUDA(cudaEventCreate(&e1));
     double best = 1e30;
-    int best_bn = -1, best_grid = B->num_sms;
+    int best_bn = -1, best_grid = B->num_sms, best_ks = 1;
     int rc = PSF_OK;
     for (int v : variants) {
         if (v < need_bn) continue;
         for (int g : grids) {
-            for (int rep = 0; rc == PSF_OK && rep < 2; ++rep) {
-                rc = psf::launch_batch_gemm(B->contract, 0, v, g, B->stream);
-                if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, v, g, B->stream);
+            for (int ks : splits) {
+                B->bn_max = v;
+                B->gemm_ctas = g;
+                B->ksplit = ks;
+                fill_gemm_args(B);
+                if ((rc = upload_tables(B)) != PSF_OK) break;
+                for (int rep = 0; rc == PSF_OK && rep < 2; ++rep) rc = launch_tc_part(B, B->stream, B->use_fused);
+                const int reps = 5;
+                cudaEventRecord(e0, B->stream);
+                for (int rep = 0; rc == PSF_OK && rep < reps; ++rep) rc = launch_tc_part(B, B->stream, B->use_fused);
+                cudaEventRecord(e1, B->stream);
+                cudaError_t e = cudaEventSynchronize(e1);
+                if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "autotune");
+                if (rc == PSF_OK) rc = check_device_error(B);
+                if (rc != PSF_OK) break;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms / reps < best) {
+                    best = ms / reps;
+                    best_bn = v;
+                    best_grid = g;
+                    best_ks = ks;
+                }
             }
-            const int reps = 5;
-            cudaEventRecord(e0, B->stream);
-            for (int rep = 0; rc == PSF_OK && rep < reps; ++rep) {
-                rc = psf::launch_batch_gemm(B->contract, 0, v, g, B->stream);
-                if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, v, g, B->stream);
-            }
-            cudaEventRecord(e1, B->stream);
-            cudaError_t e = cudaEventSynchronize(e1);
-            if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "autotune");
-            if (rc == PSF_OK) rc = check_device_error(B);
             if (rc != PSF_OK) break;
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms / reps < best) {
-                best = ms / reps;
-                best_bn = v;
-                best_grid = g;
-            }
         }
         if (rc != PSF_OK) break;
     }
@@ -401,15 +449,15 @@ int autotune(psf_batch *B, int need_bn)
     if (rc != PSF_OK) return rc;
     B->bn_max = best_bn;
     B->gemm_ctas = best_grid;
+    B->ksplit = best_ks;
     B->tuned_ms = best;
-    return PSF_OK;
+    fill_gemm_args(B);
+    return upload_tables(B);
 }
 
 int launch_step(psf_batch *B, cudaStream_t st)
 {
-    PSF_CHECK(psf::launch_batch_gemm(B->contract, 0, B->bn_max, B->gemm_ctas, st));
-    PSF_CHECK(psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st));
-    PSF_CHECK(psf::launch_batch_gemm(B->recon, 1, B->bn_max, B->gemm_ctas, st));
+    PSF_CHECK(launch_tc_part(B, st, B->use_fused));
     PSF_CHECK(psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_prefix, B->n_slots(), B->trace_ctas, st));
     return PSF_OK;
 }
@@ -489,6 +537,9 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
                 return fail(PSF_ERR_INVALID, "active face id out of range");
         need_bn = std::max(need_bn, (int)round_up(bb.slots, 16));
     }
+    if (cfg->contraction_ksplit != 0 && cfg->contraction_ksplit != 1 && cfg->contraction_ksplit != 2 &&
+        cfg->contraction_ksplit != 4)
+        return fail(PSF_ERR_INVALID, "contraction_ksplit must be 0, 1, 2 or 4");
     if (cfg->gemm_columns != 0 && cfg->gemm_columns < need_bn)
         return fail(PSF_ERR_INVALID, "gemm_columns is smaller than the slots of a basis");
 
@@ -509,7 +560,8 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
     e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaStreamCreate"));
     int rc = PSF_OK;
-    if ((rc = B->alloc(&B->d_err, 1)) != PSF_OK) return bail(rc);
+    if ((rc = B->alloc(&B->d_err, 1)) != PSF_OK || (rc = B->alloc(&B->grid_bar, 1)) != PSF_OK) return bail(rc);
+    B->use_fused = cfg->unfused == 0;
     if ((e = cudaMemsetAsync(B->d_err, 0, sizeof(int), B->stream)) != cudaSuccess)
         return bail(psf::cuda_fail(e, "cudaMemset"));
 
@@ -571,8 +623,8 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
         o.temp = temp;
         o.temp_bytes = tmp;
     }
-    if ((rc = upload_tables(B)) != PSF_OK || (rc = upload_prefix(B)) != PSF_OK) return bail(rc);
     fill_gemm_args(B);
+    if ((rc = upload_tables(B)) != PSF_OK || (rc = upload_prefix(B)) != PSF_OK) return bail(rc);
     B->trace_ctas = psf::batch_trace_grid(B->num_sms);
     B->gemm_ctas = cfg->gemm_ctas > 0 ? cfg->gemm_ctas : B->num_sms;
     if (cfg->gemm_columns != 0) {
@@ -582,6 +634,11 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
         if (cfg->gemm_ctas > 0) B->gemm_ctas = cfg->gemm_ctas;
     } else {
         B->bn_max = need_bn <= 64 ? 64 : (need_bn <= 128 ? 128 : 256);
+    }
+    if (cfg->contraction_ksplit > 0) {
+        B->ksplit = cfg->contraction_ksplit;
+        fill_gemm_args(B);
+        if ((rc = upload_tables(B)) != PSF_OK) return bail(rc);
     }
     *out = B;
     return PSF_OK;
@@ -602,9 +659,10 @@ int psf_batch_info_get(psf_batch *B, psf_batch_info *info)
     info->gemm_columns = B->bn_max;
     info->gemm_ctas = B->gemm_ctas;
     info->trace_ctas = B->trace_ctas;
-    info->kernels_per_step = 4;
+    info->kernels_per_step = B->use_fused ? 2 : 4;
     info->device_bytes = B->bytes;
     info->tuned_ms = B->tuned_ms;
+    info->contraction_ksplit = B->ksplit;
     return PSF_OK;
 }
 
@@ -672,6 +730,8 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
         PSF_CHECK(psf::launch_order_particles(particle_view(B, basis, slot, inst->n_particles), B->order, st));
     }
     PSF_CHECK(upload_prefix(B));
+    // A fused step starts from the contraction partials of the current state.
+    if (B->use_fused) PSF_CHECK(psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, st));
     PSF_CUDA(cudaStreamSynchronize(st));
     return PSF_OK;
 }
@@ -802,36 +862,59 @@ int psf_batch_get_steps(psf_batch *B, int32_t basis, int32_t slot, int64_t *step
     return PSF_OK;
 }
 
-int psf_batch_profile_step(psf_batch *B, double *kernel_ms, int32_t n)
+static int profile(psf_batch *B, double *kernel_ms, int32_t n, bool fused)
 {
-    if (!B || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
-    if (n < 4) return fail(PSF_ERR_INVALID, "kernel_ms needs 4 slots");
+    const int nk = fused ? 2 : 4;
+    if (n < nk) return fail(PSF_ERR_INVALID, "kernel_ms has fewer slots than launches per step");
     PSF_CUDA(cudaSetDevice(B->device));
     cudaEvent_t ev[5];
-    for (int i = 0; i < 5; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
+    for (int i = 0; i <= nk; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
     cudaStream_t st = B->stream;
     int rc = PSF_OK;
     cudaEventRecord(ev[0], st);
-    rc = psf::launch_batch_gemm(B->contract, 0, B->bn_max, B->gemm_ctas, st);
-    cudaEventRecord(ev[1], st);
-    if (rc == PSF_OK) rc = psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st);
-    cudaEventRecord(ev[2], st);
-    if (rc == PSF_OK) rc = psf::launch_batch_gemm(B->recon, 1, B->bn_max, B->gemm_ctas, st);
-    cudaEventRecord(ev[3], st);
+    if (fused) {
+        rc = launch_tc_part(B, st, true);
+        cudaEventRecord(ev[1], st);
+    } else {
+        rc = psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, st);
+        cudaEventRecord(ev[1], st);
+        if (rc == PSF_OK) rc = psf::launch_batch_state(B->d_groups, B->d_slots, B->n_slots(), st);
+        cudaEventRecord(ev[2], st);
+        if (rc == PSF_OK) rc = psf::launch_batch_step_tc(B->recon, B->bn_max, B->gemm_ctas, st);
+        cudaEventRecord(ev[3], st);
+    }
     if (rc == PSF_OK)
         rc = psf::launch_batch_trace(B->d_groups, B->d_slots, B->d_prefix, B->n_slots(), B->trace_ctas, st);
-    cudaEventRecord(ev[4], st);
+    cudaEventRecord(ev[nk], st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");
-    for (int i = 0; rc == PSF_OK && i < 4; ++i) {
+    for (int i = 0; rc == PSF_OK && i < nk; ++i) {
         float ms = 0.f;
         e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
         if (e != cudaSuccess) rc = psf::cuda_fail(e, "cudaEventElapsedTime");
         kernel_ms[i] = ms;
     }
-    for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+    for (int i = 0; i <= nk; ++i) cudaEventDestroy(ev[i]);
     if (rc == PSF_OK) rc = check_device_error(B);
     return rc;
+}
+
+int psf_batch_profile_step(psf_batch *B, double *kernel_ms, int32_t n)
+{
+    if (!B || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
+    return profile(B, kernel_ms, n, B->use_fused);
+}
+
+int psf_batch_profile_phases(psf_batch *B, double *kernel_ms, int32_t n)
+{
+    if (!B || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
+    PSF_CHECK(profile(B, kernel_ms, n, false));
+    // A fused batch keeps the partials of its current state between steps.
+    if (B->use_fused) {
+        PSF_CHECK(psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, B->stream));
+        PSF_CUDA(cudaStreamSynchronize(B->stream));
+    }
+    return PSF_OK;
 }
 
 int psf_batch_device_status(psf_batch *B, int32_t *code)

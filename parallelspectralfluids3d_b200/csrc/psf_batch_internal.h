@@ -15,6 +15,7 @@ constexpr int BATCH_MAX_GROUPS = 6;   // distinct bases in one batch
 constexpr int BATCH_MAX_SLOTS = 256;  // instance slots per basis (one MMA N tile)
 constexpr int BATCH_MAX_ALL_SLOTS = BATCH_MAX_GROUPS * BATCH_MAX_SLOTS;
 constexpr int GEMM_THREADS = 192;     // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int GEMM_MAX_KSPLIT = 4;
 
 // One basis inside a GEMM launch: A operand (C or Phi) and B operand (the
 // slots' coefficient vectors), both BF16 hi/lo pairs, K-major, 128-byte
@@ -22,27 +23,42 @@ constexpr int GEMM_THREADS = 192;     // warp 0 TMA, warp 1 MMA, warps 2-5 epilo
 struct alignas(64) GemmGroup {
     CUtensorMap tmA;        // 4D (k inner 64, rows 128, hi/lo 2, outer 1)
     CUtensorMap tmB;        // 3D (k inner 64, bn rows, hi/lo 2)
-    int tiles;              // 128-row tiles of this basis
+    int tiles;              // work units of this basis: 128-row tiles x K splits
     int m_inner;            // row tiles per outer index (contraction: a-tiles per mode k)
     int k_chunks;           // K / 64
+    int ksplit;             // K ranges per row tile (each writes its own partial sums)
+    int kc_per;             // K chunks per range
     int bn;                 // MMA N: slots rounded up to 16
     uint32_t tx_bytes;      // bytes one pipeline stage receives
     int cap;                // slots in use (columns)
     int n_rows;             // valid rows: N (contraction) or F_act (reconstruction)
     int ldw;                // row stride of w (= the basis' N)
     const float *wf;        // contraction: FP32 copy of the state [cap][ldw]
-    double *dwpart;         // contraction: partials [((k*m_inner + at)*4 + q)][cap]
+    double *dwpart;         // contraction: partials [slot][k][nparts] (a-tile, K range, warp)
+    int nparts;             // contraction: partials per (slot, k)
     long long n_faces;
     const int32_t *pair_dst;  // reconstruction: [n_rows][2] float slots in a slot's face pairs
     float *pairs;           // reconstruction: per-voxel face pairs [cap][3V] (float2)
     long long pair_floats;  // 6V: floats per slot in pairs
 };
 
-struct GemmArgs {
-    GemmGroup g[BATCH_MAX_GROUPS];
+struct GroupDev;
+struct SlotDev;
+
+// Arguments of one tensor-core launch: contraction units [0, c_tiles) over
+// g[0 .. n_groups), reconstruction units over g[n_groups .. 2 n_groups).
+// A fused launch (cooperative) runs the state update between the two.
+struct StepArgs {
+    GemmGroup g[2 * BATCH_MAX_GROUPS];
     int n_groups;
-    int total_tiles;
-    int *err;  // device error word (bounded waits)
+    int c_tiles;
+    int r_tiles;
+    int fused;
+    int *err;                 // device error word (bounded waits)
+    unsigned int *grid_bar;   // grid barrier counter, zeroed before each fused launch
+    const GroupDev *groups;   // state update of a fused launch
+    SlotDev *slots;
+    int n_slots;
 };
 
 // Per-slot parameters and counters, in device memory.
@@ -70,6 +86,7 @@ struct SlotDev {
 struct GroupDev {
     GridDev grid;
     int N, Nj, cap, bn, a_tiles, slot_base;
+    int nparts;           // contraction partials per mode: a_tiles x ksplit x 4
     long long n_faces, pmax;
     double *w;            // [cap][N]
     float *wf;            // [cap][N] FP32 copy of w (contraction epilogue)
@@ -87,7 +104,8 @@ struct GroupDev {
 // Launchers (psf_batch.cu).  `bn_max` selects the kernel variant (64, 128 or
 // 256 MMA columns per accumulator); `grid` the number of persistent CTAs.
 int batch_gemm_smem_bytes(int bn_max);
-int launch_batch_gemm(const GemmArgs &args, int epilogue, int bn_max, int grid, cudaStream_t st);
+int launch_batch_step_tc(const StepArgs &args, int bn_max, int grid, cudaStream_t st);
+int max_fused_grid(int bn_max, int num_sms);
 int launch_batch_state(const GroupDev *groups, SlotDev *slots, int n_slots, cudaStream_t st);
 // prefix[s] = particles of slots 0..s-1 (occupied slots only); n_slots + 1 entries.
 int launch_batch_trace(const GroupDev *groups, const SlotDev *slots, const long long *prefix, int n_slots, int grid,

@@ -42,9 +42,9 @@ struct TraceParams {
 // Device view of a single-instance context.
 struct PlainDev {
     int N, Np, S;
-    long long n_active, n_faces, P;
+    long long n_active, ldp, n_faces, P;
     const float *C;      // [N][N][Np]
-    const float *phi;    // [n_active][Np], signed, face-major (rows of 16-byte multiples)
+    const float *phiT;   // [N][ldp], signed, mode-major
     const int32_t *faces;
     double *w, *dwpart;
     const double *lam, *force;

@@ -30,6 +30,8 @@ enum : int {
     ERR_WAIT_ACC_EMPTY = 4,  // MMA warp waited too long for a drained accumulator
     ERR_WAIT_DRAIN = 5,      // producer waited too long for its last copies at exit
     ERR_TMEM_ALLOC = 6,      // TMEM allocation returned an unusable address
+    ERR_WAIT_STATE = 7,      // producer waited too long for the state update of a fused step
+    ERR_GRID_SYNC = 8,       // a grid barrier of a fused step timed out
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)

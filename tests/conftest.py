@@ -67,3 +67,11 @@ def rel_err(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="session")
+def medium_basis(make_basis):
+    """12^3 box with N = 160: two 128-row tiles per mode and three 64-wide K chunks in the GEMMs."""
+    from parallelspectralfluids3d_b200.domain import box_domain
+
+    return make_basis(box_domain(12), 160)

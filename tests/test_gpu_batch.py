@@ -198,3 +198,64 @@ def test_particle_pool_admission(small_bases):
         ref = _oracle(b, SPECS[1], 5)
         assert rel_err(batch.get_state(0, SPECS[1][0]), ref.w) <= W_TOL
         assert np.abs(batch.get_particles(0, SPECS[1][0])[:, :3] - ref.pos).max() / b.h <= P_TOL_VOX
+
+
+def test_multi_tile_shapes_match_oracle(medium_basis):
+    """N = 160 (2 a-tiles, 3 K chunks), 40 slots (MMA N = 48, a partial 32-column epilogue chunk)."""
+    b = medium_basis
+    specs = [(0, 160, 0.01, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 400, 21),
+             (17, 100, 0.02, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 0, 22),
+             (33, 129, 0.01, L.PSF_FLAG_RENORM | L.PSF_FLAG_FORCING, 0.0, L.PSF_RK1, 300, 23),
+             (39, 33, 0.02, L.PSF_FLAG_RENORM, 0.01, L.PSF_RK4, 0, 24)]
+    with Batch([b], slots=40, max_particles=512) as batch:
+        _fill(batch, b, specs)
+        for i in range(40):
+            if i not in (s[0] for s in specs):
+                w0 = initial_coefficients(int(40 + (i * 7) % 120), 100 + i)
+                batch.set_instance(0, i, w0, L.make_params(dt=0.01, integrator=L.PSF_RK4))
+        batch.step(15)
+        for spec in specs:
+            ref = _oracle(b, spec, 15)
+            assert rel_err(batch.get_state(0, spec[0]), ref.w) <= W_TOL, spec
+            if spec[6]:
+                p = batch.get_particles(0, spec[0])
+                assert np.abs(p[:, :3] - ref.pos).max() / b.h <= P_TOL_VOX, spec
+        u = batch.get_velocity(0, specs[0][0])
+    ref1 = _oracle(b, specs[0], 15)
+    assert np.abs(u - ref1.u).max() <= U_TOL * np.abs(ref1.u).max()
+
+
+@pytest.mark.parametrize("ksplit", [2, 4])
+def test_contraction_k_splits_agree(medium_basis, ksplit):
+    """Splitting the contraction's K range per tile changes only the FP32 summation order."""
+    b = medium_basis
+    specs = [(0, 160, 0.01, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 0, 31), (5, 77, 0.02, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 0, 32)]
+    outs = []
+    for ks in (1, ksplit):
+        with Batch([b], slots=8, max_particles=256, autotune=False, ksplit=ks) as batch:
+            assert batch.info()["contraction_ksplit"] == ks
+            _fill(batch, b, specs)
+            batch.step(10)
+            outs.append([batch.get_state(0, s[0]) for s in specs])
+    for spec, w1, w2 in zip(specs, outs[0], outs[1]):
+        assert rel_err(w2, w1) <= 1e-6
+        assert rel_err(w2, _oracle(b, spec, 10).w) <= W_TOL
+
+
+def test_fused_step_equals_three_launches(medium_basis):
+    """One cooperative launch (contraction, state update, reconstruction) against three launches."""
+    b = medium_basis
+    specs = [(0, 160, 0.01, L.PSF_FLAG_RENORM, 0.0, L.PSF_RK4, 300, 41),
+             (3, 90, 0.02, L.PSF_FLAG_RENORM | L.PSF_FLAG_DECAY_NEG, 0.03, L.PSF_RK1, 200, 42)]
+    outs = []
+    for fused in (True, False):
+        with Batch([b], slots=5, max_particles=512, fused=fused) as batch:
+            assert batch.info()["kernels_per_step"] == (2 if fused else 4)
+            _fill(batch, b, specs)
+            batch.step(12)
+            assert batch.device_status() == 0
+            outs.append([(batch.get_state(0, s[0]), batch.get_particles(0, s[0])) for s in specs])
+    for spec, (w1, p1), (w2, p2) in zip(specs, outs[0], outs[1]):
+        assert rel_err(w1, w2) <= 1e-10
+        assert np.abs(p1[:, :3] - p2[:, :3]).max() / b.h <= 1e-5
+        assert rel_err(w1, _oracle(b, spec, 12).w) <= W_TOL
