@@ -88,6 +88,18 @@ int psf_batch_info_get(psf_batch *b, psf_batch_info *info);
 int psf_batch_set_instance(psf_batch *b, int32_t basis, int32_t slot, const psf_instance_desc *inst);
 int psf_batch_clear_instance(psf_batch *b, int32_t basis, int32_t slot);
 
+/* The same for n placements or removals with one synchronisation; status[i]
+ * receives each placement's own result (PSF_ERR_NOMEM when its particles do
+ * not fit the pool, and so on). */
+int psf_batch_set_instances(psf_batch *b, int32_t n, const int32_t *basis, const int32_t *slot,
+                            const psf_instance_desc *const *inst, int32_t *status);
+int psf_batch_clear_instances(psf_batch *b, int32_t n, const int32_t *basis, const int32_t *slot);
+
+/* Copy the state (w[i], n_modes doubles) and the particles (xyzw[i], in the
+ * caller's original order) of n occupied slots; either pointer may be NULL. */
+int psf_batch_read_instances(psf_batch *b, int32_t n, const int32_t *basis, const int32_t *slot, double *const *w,
+                             float *const *xyzw);
+
 /* Free particles in the pool, and the largest contiguous free range. */
 int psf_batch_pool_free(psf_batch *b, int64_t *free_particles, int64_t *largest_range);
 

@@ -71,6 +71,9 @@ typedef struct psf_engine_stats {
     int64_t device_bytes;     /* held by the engine's batch */
     int64_t rollout_bytes;    /* of which charged to admitted rollouts */
     double t_now;
+    double step_s;            /* worker wall time in step launches and their synchronisation */
+    double admit_s;           /* worker wall time placing admitted rollouts */
+    double retire_s;          /* worker wall time copying out and clearing finished rollouts */
 } psf_engine_stats;
 
 int psf_engine_create(const psf_engine_config *cfg, int device, psf_engine **out);

@@ -14,6 +14,7 @@ BATCH_EXPORTS = (
     "psf_batch_clear_instance", "psf_batch_step", "psf_batch_sync", "psf_batch_get_stream",
     "psf_batch_get_state", "psf_batch_get_particles", "psf_batch_get_velocity", "psf_batch_get_steps",
     "psf_batch_profile_step", "psf_batch_profile_phases", "psf_batch_device_status", "psf_batch_pool_free",
+    "psf_batch_set_instances", "psf_batch_clear_instances", "psf_batch_read_instances",
 )
 
 
@@ -83,3 +84,7 @@ def declare(lib) -> None:
     lib.psf_batch_profile_phases.argtypes = [vp, ct.POINTER(ct.c_double), i32]
     lib.psf_batch_device_status.argtypes = [vp, ct.POINTER(i32)]
     lib.psf_batch_pool_free.argtypes = [vp, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]
+    ip = ct.POINTER(i32)
+    lib.psf_batch_set_instances.argtypes = [vp, i32, ip, ip, ct.POINTER(ct.POINTER(InstanceDesc)), ip]
+    lib.psf_batch_clear_instances.argtypes = [vp, i32, ip, ip]
+    lib.psf_batch_read_instances.argtypes = [vp, i32, ip, ip, ct.POINTER(vp), ct.POINTER(vp)]

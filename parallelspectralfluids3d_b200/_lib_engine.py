@@ -53,7 +53,8 @@ class RequestInfo(ct.Structure):
 class EngineStats(ct.Structure):
     _fields_ = [(n, ct.c_int64) for n in (
         "submitted", "admitted", "completed", "queued", "active", "instance_steps", "particle_steps",
-        "step_launches", "budget_refusals", "device_bytes", "rollout_bytes")] + [("t_now", ct.c_double)]
+        "step_launches", "budget_refusals", "device_bytes", "rollout_bytes")] + [
+        (n, ct.c_double) for n in ("t_now", "step_s", "admit_s", "retire_s")]
 
 
 def declare(lib) -> None:

@@ -666,7 +666,16 @@ int psf_batch_info_get(psf_batch *B, psf_batch_info *info)
     return PSF_OK;
 }
 
-int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_instance_desc *inst)
+}  // extern "C"
+
+namespace {
+
+// Place one instance without finishing the slot tables: the caller uploads
+// the prefix sums, primes the contraction and synchronises once for a group
+// of placements.  Host rows given to the asynchronous copies are kept in
+// `keep` until then.
+int set_one(psf_batch *B, int32_t basis, int32_t slot, const psf_instance_desc *inst,
+            std::vector<std::vector<double>> &keep)
 {
     int sg = 0;
     PSF_CHECK(slot_index(B, basis, slot, &sg));
@@ -685,7 +694,6 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
     if ((p.flags & PSF_FLAG_FORCING) && !inst->forcing)
         return fail(PSF_ERR_INVALID, "PSF_FLAG_FORCING is set but forcing is null");
     if (inst->steps < 0) return fail(PSF_ERR_INVALID, "steps must be >= 0");
-    PSF_CUDA(cudaSetDevice(B->device));
     cudaStream_t st = B->stream;
     // Particle range: give back the slot's old one, then take a new one.
     psf::SlotDev &s = B->slots[(size_t)sg];
@@ -700,15 +708,16 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
         s.active = 0;
         s.n_particles = 0;
         PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, st));
-        PSF_CHECK(upload_prefix(B));
         return fail(PSF_ERR_NOMEM, "the particle pool has no free range for this instance");
     }
     B->slot_units[(size_t)sg] = units;
-    std::vector<double> row((size_t)G.N, 0.0), frow((size_t)G.N, 0.0);
-    std::memcpy(row.data(), inst->w0, (size_t)inst->n_modes * 8);
-    if (inst->forcing) std::memcpy(frow.data(), inst->forcing, (size_t)inst->n_modes * 8);
-    PSF_CUDA(cudaMemcpyAsync(G.w + (size_t)slot * G.N, row.data(), row.size() * 8, cudaMemcpyHostToDevice, st));
-    PSF_CUDA(cudaMemcpyAsync(G.force + (size_t)slot * G.N, frow.data(), frow.size() * 8, cudaMemcpyHostToDevice, st));
+    keep.emplace_back((size_t)(2 * G.N), 0.0);
+    std::vector<double> &rows = keep.back();
+    std::memcpy(rows.data(), inst->w0, (size_t)inst->n_modes * 8);
+    if (inst->forcing) std::memcpy(rows.data() + G.N, inst->forcing, (size_t)inst->n_modes * 8);
+    PSF_CUDA(cudaMemcpyAsync(G.w + (size_t)slot * G.N, rows.data(), (size_t)G.N * 8, cudaMemcpyHostToDevice, st));
+    PSF_CUDA(cudaMemcpyAsync(G.force + (size_t)slot * G.N, rows.data() + G.N, (size_t)G.N * 8,
+                             cudaMemcpyHostToDevice, st));
     s.active = 1;
     s.poff = start * 256;
     s.target = (unsigned long long)inst->steps;
@@ -729,33 +738,102 @@ int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_
                                  cudaMemcpyHostToDevice, st));
         PSF_CHECK(psf::launch_order_particles(particle_view(B, basis, slot, inst->n_particles), B->order, st));
     }
-    PSF_CHECK(upload_prefix(B));
-    // A fused step starts from the contraction partials of the current state.
-    if (B->use_fused) PSF_CHECK(psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, st));
-    PSF_CUDA(cudaStreamSynchronize(st));
     return PSF_OK;
+}
+
+// After placements: new prefix sums, the contraction partials a fused step
+// starts from, and one synchronisation.
+int finish_placements(psf_batch *B)
+{
+    PSF_CHECK(upload_prefix(B));
+    if (B->use_fused) PSF_CHECK(psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, B->stream));
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return PSF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psf_batch_set_instance(psf_batch *B, int32_t basis, int32_t slot, const psf_instance_desc *inst)
+{
+    if (!B) return fail(PSF_ERR_INVALID, "null batch");
+    PSF_CUDA(cudaSetDevice(B->device));
+    std::vector<std::vector<double>> keep;
+    const int rc = set_one(B, basis, slot, inst, keep);
+    const std::string msg = psf::g_last_error;
+    const int rc2 = finish_placements(B);
+    if (rc != PSF_OK) return fail(rc, msg);
+    return rc2;
+}
+
+int psf_batch_set_instances(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot,
+                            const psf_instance_desc *const *inst, int32_t *status)
+{
+    if (!B || n < 0 || (n > 0 && (!basis || !slot || !inst || !status))) return fail(PSF_ERR_INVALID, "null argument");
+    PSF_CUDA(cudaSetDevice(B->device));
+    std::vector<std::vector<double>> keep;
+    for (int32_t i = 0; i < n; ++i) status[i] = set_one(B, basis[i], slot[i], inst[i], keep);
+    return finish_placements(B);
+}
+
+int psf_batch_clear_instances(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot)
+{
+    if (!B || n < 0 || (n > 0 && (!basis || !slot))) return fail(PSF_ERR_INVALID, "null argument");
+    PSF_CUDA(cudaSetDevice(B->device));
+    bool synced = false;
+    for (int32_t i = 0; i < n; ++i) {
+        int sg = 0;
+        PSF_CHECK(slot_index(B, basis[i], slot[i], &sg));
+        HostGroup &G = B->groups[(size_t)basis[i]];
+        psf::SlotDev &s = B->slots[(size_t)sg];
+        if (B->slot_units[(size_t)sg] > 0) {
+            if (!synced) PSF_CUDA(cudaStreamSynchronize(B->stream));
+            synced = true;
+            B->pool.release(s.poff / 256, B->slot_units[(size_t)sg]);
+            B->slot_units[(size_t)sg] = 0;
+        }
+        s.active = 0;
+        s.n_particles = 0;
+        s.stepped = 0;
+        PSF_CUDA(cudaMemsetAsync(G.w + (size_t)slot[i] * G.N, 0, (size_t)G.N * 8, B->stream));
+        PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, B->stream));
+        PSF_CHECK(psf::launch_batch_pack(B->d_groups, B->d_slots, sg, B->stream));
+    }
+    return upload_prefix(B);
 }
 
 int psf_batch_clear_instance(psf_batch *B, int32_t basis, int32_t slot)
 {
-    int sg = 0;
-    PSF_CHECK(slot_index(B, basis, slot, &sg));
+    return psf_batch_clear_instances(B, 1, &basis, &slot);
+}
+
+int psf_batch_read_instances(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot, double *const *w,
+                             float *const *xyzw)
+{
+    if (!B || n < 0 || (n > 0 && (!basis || !slot || !w || !xyzw))) return fail(PSF_ERR_INVALID, "null argument");
     PSF_CUDA(cudaSetDevice(B->device));
-    HostGroup &G = B->groups[(size_t)basis];
-    psf::SlotDev &s = B->slots[(size_t)sg];
-    if (B->slot_units[(size_t)sg] > 0) {
-        PSF_CUDA(cudaStreamSynchronize(B->stream));
-        B->pool.release(s.poff / 256, B->slot_units[(size_t)sg]);
-        B->slot_units[(size_t)sg] = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        int sg = 0;
+        PSF_CHECK(slot_index(B, basis[i], slot[i], &sg));
+        const psf::SlotDev &s = B->slots[(size_t)sg];
+        if (!s.active) return fail(PSF_ERR_STATE, "slot is empty");
+        HostGroup &G = B->groups[(size_t)basis[i]];
+        if (w[i])
+            PSF_CUDA(cudaMemcpyAsync(w[i], G.w + (size_t)slot[i] * G.N, (size_t)s.n_modes * 8, cudaMemcpyDeviceToHost,
+                                     B->stream));
+        if (xyzw[i] && s.n_particles > 0) {
+            // Scatter back to the caller's order in a per-slot region of the
+            // ordering scratch is not possible for several slots at once, so
+            // each slot is un-ordered into the staging buffer and copied.
+            PSF_CHECK(psf::launch_unorder_particles(particle_view(B, basis[i], slot[i], s.n_particles), B->order,
+                                                    B->stream));
+            PSF_CUDA(cudaMemcpyAsync(xyzw[i], B->order.staging, (size_t)s.n_particles * 16, cudaMemcpyDeviceToHost,
+                                     B->stream));
+        }
     }
-    s.active = 0;
-    s.n_particles = 0;
-    s.stepped = 0;
-    PSF_CUDA(cudaMemsetAsync(G.w + (size_t)slot * G.N, 0, (size_t)G.N * 8, B->stream));
-    PSF_CUDA(cudaMemcpyAsync(B->d_slots + sg, &s, sizeof(s), cudaMemcpyHostToDevice, B->stream));
-    PSF_CHECK(psf::launch_batch_pack(B->d_groups, B->d_slots, sg, B->stream));
-    PSF_CHECK(upload_prefix(B));
-    return PSF_OK;
+    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    return check_device_error(B);
 }
 
 int psf_batch_pool_free(psf_batch *B, int64_t *free_particles, int64_t *largest_range)

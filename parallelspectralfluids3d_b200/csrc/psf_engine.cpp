@@ -140,8 +140,14 @@ int psf_engine::admit_round()
             it = queue.erase(it);
         }
     }
-    for (const ReqPtr &r : picked) {
-        psf_instance_desc d{};
+    if (picked.empty()) return PSF_OK;
+    std::vector<psf_instance_desc> descs(picked.size());
+    std::vector<const psf_instance_desc *> dptr(picked.size());
+    std::vector<int32_t> bas(picked.size()), slt(picked.size()), status(picked.size(), PSF_OK);
+    for (size_t i = 0; i < picked.size(); ++i) {
+        const ReqPtr &r = picked[i];
+        psf_instance_desc &d = descs[i];
+        d = psf_instance_desc{};
         d.n_modes = r->n_modes;
         d.params = r->params;
         d.w0 = r->w0.data();
@@ -149,7 +155,20 @@ int psf_engine::admit_round()
         d.particles = r->parts.empty() ? nullptr : r->parts.data();
         d.n_particles = (int64_t)r->parts.size() / 4;
         d.steps = r->steps;
-        const int rc = psf_batch_set_instance(batch, r->basis, r->slot, &d);
+        dptr[i] = &d;
+        bas[i] = r->basis;
+        slt[i] = r->slot;
+    }
+    const double ta = now();
+    const int rc_all = psf_batch_set_instances(batch, (int32_t)picked.size(), bas.data(), slt.data(), dptr.data(),
+                                               status.data());
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        st.admit_s += now() - ta;
+    }
+    for (size_t i = 0; i < picked.size(); ++i) {
+        const ReqPtr &r = picked[i];
+        const int rc = rc_all != PSF_OK ? rc_all : status[i];
         if (rc == PSF_ERR_NOMEM) {
             // No contiguous particle range yet: back to the head of the queue.
             std::lock_guard<std::mutex> lock(mu);
@@ -188,13 +207,16 @@ int psf_engine::step_round()
     int64_t most = 0;
     for (const ReqPtr &r : running) most = std::max(most, r->remaining);
     const int k = (int)std::min<int64_t>(chunk, most);
+    const double ts = now();
     int rc = psf_batch_step(batch, k);
     if (rc == PSF_OK) rc = psf_batch_sync(batch);
     if (rc != PSF_OK) return rc;
+    const double t_stepped = now();
     std::vector<ReqPtr> finished;
     {
         std::lock_guard<std::mutex> lock(mu);
         st.step_launches += k;
+        st.step_s += t_stepped - ts;
         for (const ReqPtr &r : running) {
             const int64_t d = std::min<int64_t>(k, r->remaining);
             r->remaining -= d;
@@ -203,18 +225,32 @@ int psf_engine::step_round()
             if (r->remaining == 0) finished.push_back(r);
         }
     }
-    for (const ReqPtr &r : finished) {
+    if (finished.empty()) return PSF_OK;
+    std::vector<int32_t> bas(finished.size()), slt(finished.size());
+    std::vector<double *> wp(finished.size());
+    std::vector<float *> pp(finished.size());
+    for (size_t i = 0; i < finished.size(); ++i) {
+        const ReqPtr &r = finished[i];
         r->w_out.resize((size_t)r->n_modes);
         r->p_out.resize(r->parts.size());
-        const int64_t P = (int64_t)r->parts.size() / 4;
-        int e = psf_batch_get_state(batch, r->basis, r->slot, r->w_out.data(), r->n_modes);
-        if (e == PSF_OK) e = psf_batch_get_particles(batch, r->basis, r->slot, r->p_out.data(), P);
-        if (e == PSF_OK) e = psf_batch_clear_instance(batch, r->basis, r->slot);
+        bas[i] = r->basis;
+        slt[i] = r->slot;
+        wp[i] = r->w_out.data();
+        pp[i] = r->p_out.empty() ? nullptr : r->p_out.data();
+    }
+    const double tr = now();
+    int e = psf_batch_read_instances(batch, (int32_t)finished.size(), bas.data(), slt.data(), wp.data(), pp.data());
+    if (e == PSF_OK) e = psf_batch_clear_instances(batch, (int32_t)finished.size(), bas.data(), slt.data());
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        st.retire_s += now() - tr;
+    }
+    for (const ReqPtr &r : finished) {
         r->parts.clear();
         r->parts.shrink_to_fit();
         finish(r, e);
-        if (e != PSF_OK) return e;
     }
+    if (e != PSF_OK) return e;
     return PSF_OK;
 }
 
