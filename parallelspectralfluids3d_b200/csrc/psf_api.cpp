@@ -261,6 +261,8 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     const psf_grid &g = b->grid;
     if (g.dims[0] == 0 || g.dims[1] == 0 || g.dims[2] == 0 || !(g.resolution > 0.0))
         return fail(PSF_ERR_INVALID, "grid dims and resolution must be positive");
+    if (g.dims[0] > 1023 || g.dims[1] > 1023 || g.dims[2] > 1023)
+        return fail(PSF_ERR_UNSUPPORTED, "grid dims above 1023 voxels per axis");
     if (b->n_modes < 1 || b->n_modes > psf::PSF_MAX_MODES)
         return fail(PSF_ERR_UNSUPPORTED, "n_modes must be in [1, 1024]");
     if (b->n_active < 1) return fail(PSF_ERR_INVALID, "n_active must be positive");

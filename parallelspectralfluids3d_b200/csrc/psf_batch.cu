@@ -56,9 +56,12 @@ struct GemmCfg {
 };
 
 // Work unit t of a launch: contraction units first, then reconstruction units.
+// MODE 0 launches only contraction units, MODE 1 only reconstruction units,
+// MODE 2 (fused) both, so the unit kind is known at compile time except there.
+template <int MODE>
 __device__ __forceinline__ const GemmGroup &unit_group(const StepArgs &a, int t, bool &recon, int *local)
 {
-    recon = t >= a.c_tiles;
+    recon = MODE == 1 ? true : (MODE == 0 ? false : t >= a.c_tiles);
     int base = recon ? a.n_groups : 0;
     int u = recon ? t - a.c_tiles : t;
     int g = 0;
@@ -160,8 +163,8 @@ __device__ void state_update_cta(const GroupDev *__restrict__ groups, SlotDev &s
     double e1 = 0.0, e2 = 0.0;
     for (int i = et; i < N; i += 128) {
         double dw = 0.0;
-        const double *dp = G.dwpart + ((size_t)b * G.N + i) * parts;
-        for (int p = 0; p < parts; ++p) dw += dp[p];
+        const double *dp = G.dwpart + (size_t)i * parts * G.cap + b;
+        for (int p = 0; p < parts; ++p) dw += dp[(size_t)p * G.cap];
         const double wi = w[i];
         const double w1 = wi + s.dt * dw;
         w[i] = w1;
@@ -206,7 +209,7 @@ __device__ void state_update_cta(const GroupDev *__restrict__ groups, SlotDev &s
 // coefficients).  During the update the producer already loads the first
 // tiles of C and Phi, which do not depend on the state, and issues their
 // coefficient (W) loads once the barrier has passed.
-template <int BN_MAX>
+template <int BN_MAX, int MODE>
 __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __grid_constant__ StepArgs args)
 {
     using Cfg = GemmCfg<BN_MAX>;
@@ -260,14 +263,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             // Reconstruction stages whose W load waits for the state update.
             int pend_stage[STAGES], pend_kc[STAGES], pend_t[STAGES];
             int npend = 0;
-            bool w_ok = !args.fused;
+            bool w_ok = MODE != 2;
             bool ok = true;
             auto flush = [&]() -> bool {
                 if (!mbar_wait(wready, 0u, err, ERR_WAIT_STATE)) return false;
                 for (int i = 0; i < npend; ++i) {
                     bool rc;
                     int lt;
-                    const GemmGroup &G = unit_group(args, pend_t[i], rc, &lt);
+                    const GemmGroup &G = unit_group<MODE>(args, pend_t[i], rc, &lt);
                     unsigned char *sB = smem + pend_stage[i] * Cfg::STAGE_BYTES + Cfg::A_BYTES;
                     tma_load_3d(sB, &G.tmB, &full[pend_stage[i]], pend_kc[i] * 64, 0, 0);
                 }
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             for (int t = blockIdx.x; ok && t < total; t += gridDim.x) {
                 bool recon;
                 int lt;
-                const GemmGroup &G = unit_group(args, t, recon, &lt);
+                const GemmGroup &G = unit_group<MODE>(args, t, recon, &lt);
                 const Unit un = decode_unit(G, lt);
                 for (int kc = un.kc0; kc < un.kc1; ++kc) {
                     if (!mbar_wait(&empty[stage], phase ^ 1u, err, ERR_WAIT_EMPTY)) {
@@ -327,7 +330,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             for (int t = blockIdx.x; ok && t < total; t += gridDim.x) {
                 bool recon;
                 int lt;
-                const GemmGroup &G = unit_group(args, t, recon, &lt);
+                const GemmGroup &G = unit_group<MODE>(args, t, recon, &lt);
                 const Unit un = decode_unit(G, lt);
                 if (!mbar_wait(&acc_empty[abuf], aphase ^ 1u, err, ERR_WAIT_ACC_EMPTY)) break;
                 tc_fence_after();
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
         const int row = q * 32 + lane;
         int abuf = 0;
         uint32_t aphase = 0;
-        if (args.fused) {
+        if (MODE == 2) {
             // Every slot's state update (one CTA per slot), then a grid
             // barrier before any coefficient (W) load of the sweep.
             const int et = threadIdx.x - 64;
@@ -383,12 +386,15 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             if (threadIdx.x == 64) {
                 if (grid_sync(args.grid_bar, gridDim.x, err)) mbar_arrive(wready);
             }
-            epilogue_bar();  // the epilogue reads other CTAs' new state (wf) below
+            epilogue_bar();
+            // The epilogue reads other CTAs' new state (wf) below with
+            // ordinary (L1-cached) loads: order them after the barrier.
+            __threadfence();
         }
         for (int t = blockIdx.x; t < total; t += gridDim.x) {
             bool recon;
             int lt;
-            const GemmGroup &G = unit_group(args, t, recon, &lt);
+            const GemmGroup &G = unit_group<MODE>(args, t, recon, &lt);
             const Unit un = decode_unit(G, lt);
             const int outer = un.outer, inner = un.inner;
             // Contraction: the state values of this warp's rows for the first
@@ -399,7 +405,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             if (!recon) {
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
-                    wv[c] = (arow && c < G.cap) ? __ldcg(G.wf + (size_t)c * G.ldw + a_row) : 0.f;
+                    wv[c] = (arow && c < G.cap) ? G.wf[(size_t)c * G.ldw + a_row] : 0.f;
             }
             bool ok = mbar_wait(&acc_full[abuf], aphase, err, ERR_WAIT_ACC_FULL);
             ok = __all_sync(0xffffffffu, ok);
@@ -418,13 +424,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
 #pragma unroll
                         for (int c = 0; c < 32; ++c) {
                             const int b = c0 + 32 + c;
-                            wv[c] = (arow && b < G.cap) ? __ldcg(G.wf + (size_t)b * G.ldw + a_row) : 0.f;
+                            wv[c] = (arow && b < G.cap) ? G.wf[(size_t)b * G.ldw + a_row] : 0.f;
                         }
                     }
                     const float s = warp_reduce_scatter32f(y, lane);
                     const int b = c0 + lane;
                     if (b < G.cap)
-                        G.dwpart[((size_t)b * G.n_rows + outer) * G.nparts + (inner * G.ksplit + un.ks) * 4 + q] =
+                        G.dwpart[((size_t)outer * G.nparts + (inner * G.ksplit + un.ks) * 4 + q) * G.cap + b] =
                             (double)s;
                 }
             } else {
@@ -487,8 +493,8 @@ __global__ void __launch_bounds__(256) psf_batch_state(const GroupDev *__restric
     double e1 = 0.0, e2 = 0.0;
     for (int i = threadIdx.x; i < N; i += 256) {
         double dw = 0.0;
-        const double *dp = G.dwpart + ((size_t)b * G.N + i) * parts;
-        for (int p = 0; p < parts; ++p) dw += dp[p];
+        const double *dp = G.dwpart + (size_t)i * parts * G.cap + b;
+        for (int p = 0; p < parts; ++p) dw += dp[(size_t)p * G.cap];
         const double wi = w[i];
         const double w1 = wi + s.dt * dw;
         wnew[i] = w1;
@@ -599,7 +605,7 @@ int batch_gemm_smem_bytes(int bn_max)
     }
 }
 
-template <int BN>
+template <int BN, int MODE>
 static int launch_tc_t(const StepArgs &args, int grid, cudaStream_t st)
 {
     // The shared-memory limit is a per-device attribute of the kernel.
@@ -609,7 +615,7 @@ static int launch_tc_t(const StepArgs &args, int grid, cudaStream_t st)
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(configured & bit)) {
-        e = cudaFuncSetAttribute(psf_batch_step_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(psf_batch_step_tc<BN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  GemmCfg<BN>::SMEM);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(psf_batch_step_tc)");
         configured |= bit;
@@ -621,12 +627,23 @@ static int launch_tc_t(const StepArgs &args, int grid, cudaStream_t st)
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = args.fused ? 1 : 0;
+    attr[0].val.cooperative = MODE == 2 ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, psf_batch_step_tc<BN>, args);
+    e = cudaLaunchKernelEx(&cfg, psf_batch_step_tc<BN, MODE>, args);
     if (e != cudaSuccess) return cuda_fail(e, "psf_batch_step_tc launch");
     return PSF_OK;
+}
+
+template <int MODE>
+static int launch_tc_mode(const StepArgs &args, int bn_max, int grid, cudaStream_t st)
+{
+    switch (bn_max) {
+    case 64: return launch_tc_t<64, MODE>(args, grid, st);
+    case 128: return launch_tc_t<128, MODE>(args, grid, st);
+    case 256: return launch_tc_t<256, MODE>(args, grid, st);
+    }
+    return fail(PSF_ERR_UNSUPPORTED, "GEMM variant must have 64, 128 or 256 columns");
 }
 
 int launch_batch_step_tc(const StepArgs &args, int bn_max, int grid, cudaStream_t st)
@@ -640,12 +657,10 @@ int launch_batch_step_tc(const StepArgs &args, int bn_max, int grid, cudaStream_
         if (used && (args.g[g].bn > bn_max || args.g[g].bn % 16 != 0 || args.g[g].bn < 16))
             return fail(PSF_ERR_INVALID, "GEMM group N tile does not fit the kernel variant");
     }
-    switch (bn_max) {
-    case 64: return launch_tc_t<64>(args, grid, st);
-    case 128: return launch_tc_t<128>(args, grid, st);
-    case 256: return launch_tc_t<256>(args, grid, st);
-    }
-    return fail(PSF_ERR_UNSUPPORTED, "GEMM variant must have 64, 128 or 256 columns");
+    if (args.fused) return launch_tc_mode<2>(args, bn_max, grid, st);
+    if (args.r_tiles == 0) return launch_tc_mode<0>(args, bn_max, grid, st);
+    if (args.c_tiles == 0) return launch_tc_mode<1>(args, bn_max, grid, st);
+    return fail(PSF_ERR_INVALID, "an unfused launch runs either contraction or reconstruction units");
 }
 
 // Largest persistent grid a cooperative launch of the variant can hold.
@@ -655,20 +670,20 @@ int max_fused_grid(int bn_max, int num_sms)
     cudaError_t e = cudaSuccess;
     switch (bn_max) {
     case 64:
-        cudaFuncSetAttribute(psf_batch_step_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<64>::SMEM);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<64>, GEMM_THREADS,
+        cudaFuncSetAttribute(psf_batch_step_tc<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<64>::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<64, 2>, GEMM_THREADS,
                                                           GemmCfg<64>::SMEM);
         break;
     case 128:
-        cudaFuncSetAttribute(psf_batch_step_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(psf_batch_step_tc<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              GemmCfg<128>::SMEM);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<128>, GEMM_THREADS,
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<128, 2>, GEMM_THREADS,
                                                           GemmCfg<128>::SMEM);
         break;
     default:
-        cudaFuncSetAttribute(psf_batch_step_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(psf_batch_step_tc<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              GemmCfg<256>::SMEM);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<256>, GEMM_THREADS,
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_batch_step_tc<256, 2>, GEMM_THREADS,
                                                           GemmCfg<256>::SMEM);
         break;
     }

@@ -407,16 +407,20 @@ int autotune(psf_batch *B, int need_bn)
     const int variants[3] = {64, 128, 256};
     const int grids[2] = {B->num_sms, std::max(1, B->num_sms / 2)};
     const int splits[3] = {1, 2, 4};
+    const bool try_fused = B->use_fused;  // a batch created unfused stays unfused
     cudaEvent_t e0, e1;
     PSF_CUDA(cudaEventCreate(&e0));
     PSF_CUDA(cudaEventCreate(&e1));
     double best = 1e30;
     int best_bn = -1, best_grid = B->num_sms, best_ks = 1;
     int rc = PSF_OK;
+    bool best_fused = try_fused;
+    for (int fu = try_fused ? 1 : 0; fu >= 0; --fu)
     for (int v : variants) {
         if (v < need_bn) continue;
         for (int g : grids) {
             for (int ks : splits) {
+                B->use_fused = fu == 1;
                 B->bn_max = v;
                 B->gemm_ctas = g;
                 B->ksplit = ks;
@@ -438,6 +442,7 @@ int autotune(psf_batch *B, int need_bn)
                     best_bn = v;
                     best_grid = g;
                     best_ks = ks;
+                    best_fused = B->use_fused;
                 }
             }
             if (rc != PSF_OK) break;
@@ -450,6 +455,7 @@ int autotune(psf_batch *B, int need_bn)
     B->bn_max = best_bn;
     B->gemm_ctas = best_grid;
     B->ksplit = best_ks;
+    B->use_fused = best_fused;
     B->tuned_ms = best;
     fill_gemm_args(B);
     return upload_tables(B);
@@ -528,6 +534,8 @@ int psf_batch_create(const psf_batch_config *cfg, int device, psf_batch **out)
             return fail(PSF_ERR_INVALID, "basis arrays must not be null");
         if (b.grid.dims[0] == 0 || b.grid.dims[1] == 0 || b.grid.dims[2] == 0 || !(b.grid.resolution > 0.0))
             return fail(PSF_ERR_INVALID, "grid dims and resolution must be positive");
+        if (b.grid.dims[0] > 1023 || b.grid.dims[1] > 1023 || b.grid.dims[2] > 1023)
+            return fail(PSF_ERR_UNSUPPORTED, "grid dims above 1023 voxels per axis");
         const int64_t F = psf::n_faces_of(b.grid);
         const int64_t V = (int64_t)b.grid.dims[0] * b.grid.dims[1] * b.grid.dims[2];
         if (F >= (int64_t)INT32_MAX || 6 * V >= (int64_t)INT32_MAX)

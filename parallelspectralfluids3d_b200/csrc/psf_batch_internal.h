@@ -34,7 +34,7 @@ struct alignas(64) GemmGroup {
     int n_rows;             // valid rows: N (contraction) or F_act (reconstruction)
     int ldw;                // row stride of w (= the basis' N)
     const float *wf;        // contraction: FP32 copy of the state [cap][ldw]
-    double *dwpart;         // contraction: partials [slot][k][nparts] (a-tile, K range, warp)
+    double *dwpart;         // contraction: partials [k][nparts (a-tile, K range, warp)][slot]
     int nparts;             // contraction: partials per (slot, k)
     long long n_faces;
     const int32_t *pair_dst;  // reconstruction: [n_rows][2] float slots in a slot's face pairs

@@ -68,8 +68,11 @@ __device__ __forceinline__ uint32_t voxel(const GridDev &g, int x, int y, int z)
 
 // Staggered cell of a position: the clamped voxel indices of the three
 // component stencils, and the position in voxel units from the box corner.
+// `key` packs the unclamped floor indices they all derive from, so two
+// positions share a cell exactly when their keys are equal.
 struct Cell {
     int xO, yO, zO, xM, xP, yM, yP, zM, zP;
+    uint32_t keyO, keyR;
 };
 
 __device__ __forceinline__ Cell cell_of(const GridDev &g, float px, float py, float pz, float3 &gw)
@@ -91,13 +94,16 @@ __device__ __forceinline__ Cell cell_of(const GridDev &g, float px, float py, fl
     c.yP = clampi(yr + 1, 0, g.ny - 1);
     c.zM = clampi(zr, 0, g.nz - 1);
     c.zP = clampi(zr + 1, 0, g.nz - 1);
+    // Clamped indices are in [0, 1023] and xr + 1 in [0, 1024): 10 bits each.
+    c.keyO = (uint32_t)c.xO | ((uint32_t)c.yO << 10) | ((uint32_t)c.zO << 20);
+    c.keyR = (uint32_t)clampi(xr + 1, 0, 1023) | ((uint32_t)clampi(yr + 1, 0, 1023) << 10) |
+             ((uint32_t)clampi(zr + 1, 0, 1023) << 20);
     return c;
 }
 
 __device__ __forceinline__ bool same_cell(const Cell &a, const Cell &b)
 {
-    return a.xO == b.xO && a.yO == b.yO && a.zO == b.zO && a.xM == b.xM && a.xP == b.xP && a.yM == b.yM &&
-           a.yP == b.yP && a.zM == b.zM && a.zP == b.zP;
+    return a.keyO == b.keyO && a.keyR == b.keyR;
 }
 
 // The 24 face samples of a cell as 12 face pairs.

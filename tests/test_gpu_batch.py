@@ -249,7 +249,7 @@ def test_fused_step_equals_three_launches(medium_basis):
              (3, 90, 0.02, L.PSF_FLAG_RENORM | L.PSF_FLAG_DECAY_NEG, 0.03, L.PSF_RK1, 200, 42)]
     outs = []
     for fused in (True, False):
-        with Batch([b], slots=5, max_particles=512, fused=fused) as batch:
+        with Batch([b], slots=5, max_particles=512, fused=fused, autotune=False) as batch:
             assert batch.info()["kernels_per_step"] == (2 if fused else 4)
             _fill(batch, b, specs)
             batch.step(12)
