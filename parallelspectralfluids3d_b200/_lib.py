@@ -121,11 +121,12 @@ def load(path: str | None = None):
 
 
 def _extend(L):
-    """Declare the batch and engine entry points when the build has them."""
-    from . import _lib_batch, _lib_engine
+    """Declare the batch, engine and voxeliser entry points."""
+    from . import _lib_batch, _lib_engine, _lib_voxel
 
     _lib_batch.declare(L)
     _lib_engine.declare(L)
+    _lib_voxel.declare(L)
 
 
 def check(rc: int) -> None:
