@@ -40,9 +40,10 @@ def build(force: bool = False) -> str:
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
         cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-o", LIB, SRC, "-lm"]
         subprocess.run(cmd, check=True)
-    from . import voxel_oracle
+    from . import volume_oracle, voxel_oracle
 
     voxel_oracle.build(force)
+    volume_oracle.build(force)
     return LIB
 
 

@@ -121,12 +121,13 @@ def load(path: str | None = None):
 
 
 def _extend(L):
-    """Declare the batch, engine and voxeliser entry points."""
-    from . import _lib_batch, _lib_engine, _lib_voxel
+    """Declare the batch, engine, voxeliser and volume entry points."""
+    from . import _lib_batch, _lib_engine, _lib_volume, _lib_voxel
 
     _lib_batch.declare(L)
     _lib_engine.declare(L)
     _lib_voxel.declare(L)
+    _lib_volume.declare(L)
 
 
 def check(rc: int) -> None:

@@ -235,6 +235,20 @@ static int build_graph(psf_ctx *c)
     return PSF_OK;
 }
 
+int psf::context_particles(psf_ctx *c, ContextParticles *out)
+{
+    if (!c || !out) return fail(PSF_ERR_INVALID, "null argument");
+    out->device = c->device;
+    out->stream = c->stream;
+    out->parts = c->d.parts;
+    out->n = c->d.P;
+    for (int a = 0; a < 3; ++a) {
+        out->mn[a] = c->grid.aabb_min[a];
+        out->mx[a] = c->grid.aabb_max[a];
+    }
+    return PSF_OK;
+}
+
 extern "C" {
 
 int psf_abi_version(void) { return PSF_ABI_VERSION; }

@@ -83,6 +83,16 @@ void face_pair_slots(const psf_grid &g, const int32_t *faces, int64_t n_active, 
 // Tracer constants of a grid (the reference's index offsets and box).
 GridDev make_grid_dev(const psf_grid &g);
 
+// Resident particles of a single-instance context (for consumers on its device).
+struct ContextParticles {
+    int device;
+    cudaStream_t stream;
+    const float4 *parts;  // [n] in the context's storage order
+    long long n;
+    float mn[3], mx[3];   // the grid's AABB
+};
+int context_particles(psf_ctx *c, ContextParticles *out);
+
 extern thread_local std::string g_last_error;
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
