@@ -426,9 +426,11 @@ def batch_params(wl, x):
 
 
 def fill_batch(batch, wl, insts):
-    for x in insts:
-        batch.set_instance(x["basis"], x["slot"], x["w0"], batch_params(wl, x), particles=x["parts"],
-                           forcing=x["force"] if wl["force0"] else None)
+    status = batch.set_instances([
+        {"basis": x["basis"], "slot": x["slot"], "w0": x["w0"], "params": batch_params(wl, x), "particles": x["parts"],
+         "forcing": x["force"] if wl["force0"] else None} for x in insts])
+    if np.any(status != 0):
+        raise RuntimeError(f"placement failed: {sorted(set(status.tolist()))}")
 
 
 def batch_kernel_bytes(bases, slots, insts, kind):
@@ -882,13 +884,116 @@ def run_for_profiler(args):
     ctx.close()
 
 
+# ---------------------------------------------------------------- the steps before and after the path
+# Mesh voxeliser (Graphics/Model/Model.cpp:203-451) and particle density volume + ray march
+# (Solver/SolverImpl/psfsolvergpu.cpp:876-1022): not on the instance-steps/s metric; each prints
+# its own line.
+AUX_WORKLOADS = {
+    "voxel_sphere_512": "icosphere with 1,310,720 triangles (radius 0.45) voxelised at 512^3, geometric mode",
+    "volume_cloud256": "16,777,216 particles (normal cloud, sigma 0.12) splatted into 256^3 FP16 density, "
+                       "ray-marched at 1280x720 with shadow rays",
+}
+
+
+def run_aux(args):
+    """One JSON line for a voxeliser or volume workload (device time, end to end, CPU sample)."""
+    from parallelspectralfluids3d_b200 import volume as VOL
+    from parallelspectralfluids3d_b200 import voxel as VX
+
+    peak, peak_kind = measured_peak_hbm()
+    clocks = ClockSampler(0).start()
+    steps = max(1, args.steps if args.steps <= 50 else 20)
+    if args.workload == "voxel_sphere_512":
+        v, t = VX.icosphere(8, 0.45)
+        res = 0.9 / 512
+        (W, H, D), _, _ = VX.grid(v, res, VX.GEOMETRIC)
+        nvox = W * H * D
+        vz = VX.Voxelizer(len(v), len(t), nvox)
+        for _ in range(max(1, args.warmup)):
+            inside, *_ = vz.run(v, t, res, VX.GEOMETRIC)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            inside, *_ = vz.run(v, t, res, VX.GEOMETRIC)
+        e2e_s = (time.perf_counter() - t0) / steps
+        ms = vz.profile(steps)
+        vz.close()
+        words = D // 32 + 1
+        alg = 12 * len(v) + 16 * len(v) + 12 * len(t) + 48 * len(t) + 4 * words * W * H + nvox
+        line = {"metric": "voxels/s", "value": nvox / (ms / 1e3), "unit": "voxels/s", "ms_per_mesh": ms,
+                "e2e": {"value": nvox / e2e_s, "unit": "voxels/s", "h2d_bytes_per_step": 12 * len(v) + 12 * len(t),
+                        "d2h_bytes_per_step": nvox},
+                "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                             "note": "three kernels (transform, raster, unpack) timed together"},
+                "inside_voxels": int(inside.sum())}
+        if not args.no_cpu:
+            from oracle import voxel_oracle as VO
+
+            t0 = time.perf_counter()
+            want = VO.voxelize(v, t, res, VO.GEOMETRIC)
+            cpu_s = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": want.size / cpu_s, "unit": "voxels/s", "cores": 1, "kind": "port",
+                                    "sample": "the whole workload once (oracle, one thread)"}
+            line["matches_oracle"] = bool(np.array_equal(want, inside))
+    else:
+        rng = np.random.default_rng(11)
+        P = 1 << 24
+        p = np.concatenate([rng.normal(0.0, 0.12, (P, 3)), np.full((P, 1), 100.0)], 1).astype(np.float32)
+        mn = np.array([-0.5] * 3, np.float32)
+        mx = -mn
+        view = VOL.make_view(1280, 720, eye=(0.3, 0.4, 1.6))
+        vol = VOL.Volume(256)
+        for _ in range(max(1, args.warmup)):
+            vol.splat(p, mn, mx)
+            img = vol.render(view)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            vol.splat(p, mn, mx)
+            img = vol.render(view)
+        e2e_s = (time.perf_counter() - t0) / steps
+        splat_ms, render_ms = vol.profile(view, steps)
+        vol.close()
+        cells = 256 ** 3
+        alg = 16 * P + 4 * cells * 3 + 2 * cells  # particles in, counts read+cleared (+atomics), FP16 out
+        line = {"metric": "frames/s", "value": 1e3 / (splat_ms + render_ms), "unit": "frames/s",
+                "splat_ms": splat_ms, "render_ms": render_ms,
+                "e2e": {"value": 1.0 / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": 16 * P,
+                        "d2h_bytes_per_step": 16 * 1280 * 720},
+                "roofline": {"bound": "hbm", "achieved": alg / (splat_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": alg / (splat_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                             "note": "splat kernels only; the ray march is bound by L2-resident samples"},
+                "mean_transmittance": float(img[..., 3].mean())}
+        if not args.no_cpu:
+            from oracle import volume_oracle as VO
+
+            t0 = time.perf_counter()
+            d = VO.density(VO.histogram(p, mn, mx, 256))
+            cpu_splat = time.perf_counter() - t0
+            small = dict(view, width=320, height=180)
+            t0 = time.perf_counter()
+            VO.render(d, small, mn, mx)
+            cpu_px = (time.perf_counter() - t0) / (320 * 180)
+            cpu_frame = cpu_splat + cpu_px * 1280 * 720
+            line["cpu_baseline"] = {"value": 1.0 / cpu_frame, "unit": "frames/s", "cores": 1, "kind": "port",
+                                    "sample": "full splat + the same view at 320x180, scaled per pixel to 1280x720 "
+                                              "(oracle, one thread)"}
+    line.update({"n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                 "config": {"workload": args.workload, "describe": AUX_WORKLOADS[args.workload]},
+                 "gpu_launches": 3 * steps,  # transform, raster, unpack / histogram, density, render
+                 "clocks": clocks.stop()})
+    return line
+
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + [SERVE_WORKLOAD],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + [SERVE_WORKLOAD]
+                    + sorted(AUX_WORKLOADS),
                     default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu", action="store_true", help="skip the FP64 accuracy/CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched tensor-core form in the default line")
@@ -911,6 +1016,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload in AUX_WORKLOADS:
+        if rank == 0 and args.impl == "ours":
+            print(json.dumps(run_aux(args)), flush=True)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference runs this step through OpenGL, "
+                              "which is unavailable on this box; the CPU restatement is reported as cpu_baseline"}))
+        return
 
     if args.impl == "reference":
         if rank == 0:

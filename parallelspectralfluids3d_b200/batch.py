@@ -98,6 +98,47 @@ class Batch:
         self._n_modes[(basis, slot)] = n
         self._n_particles[(basis, slot)] = P
 
+    def set_instances(self, items) -> np.ndarray:
+        """Place many rollouts with one synchronisation; ``items`` holds dicts with the keys of
+        ``set_instance`` (basis, slot, w0, params, particles, forcing, n_modes, steps).  Returns each
+        placement's status (0 or a PSF_ERR_* code)."""
+        n = len(items)
+        descs = (LB.InstanceDesc * n)()
+        ptrs = (ct.POINTER(LB.InstanceDesc) * n)()
+        basis = np.zeros(n, np.int32)
+        slot = np.zeros(n, np.int32)
+        keep = []
+        for i, it in enumerate(items):
+            w0 = np.ascontiguousarray(it["w0"], dtype=np.float64)
+            keep.append(w0)
+            d = descs[i]
+            d.n_modes = int(it.get("n_modes") or w0.shape[0])
+            d.params = it["params"]
+            d.w0 = L.ptr(w0, ct.c_double)
+            if it.get("forcing") is not None:
+                f = np.ascontiguousarray(it["forcing"], dtype=np.float64)
+                keep.append(f)
+                d.forcing = L.ptr(f, ct.c_double)
+            P = 0
+            if it.get("particles") is not None:
+                p = np.ascontiguousarray(it["particles"], dtype=np.float32).reshape(-1, 4)
+                keep.append(p)
+                P = int(p.shape[0])
+                if P:
+                    d.particles = L.ptr(p, ct.c_float)
+            d.n_particles = P
+            d.steps = int(it.get("steps", 0))
+            ptrs[i] = ct.pointer(d)
+            basis[i], slot[i] = int(it["basis"]), int(it["slot"])
+        status = np.zeros(n, np.int32)
+        L.check(self.lib.psf_batch_set_instances(self.handle, n, L.ptr(basis, ct.c_int32), L.ptr(slot, ct.c_int32),
+                                                 ptrs, L.ptr(status, ct.c_int32)))
+        for i, it in enumerate(items):
+            if status[i] == 0:
+                self._n_modes[(int(basis[i]), int(slot[i]))] = int(descs[i].n_modes)
+                self._n_particles[(int(basis[i]), int(slot[i]))] = int(descs[i].n_particles)
+        return status
+
     def clear_instance(self, basis: int, slot: int) -> None:
         L.check(self.lib.psf_batch_clear_instance(self.handle, int(basis), int(slot)))
         self._n_modes.pop((basis, slot), None)
