@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(256, 3) psf_trace(float4 *__restrict__ parts, 
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
         float4 p = parts[i];
-        p = advance_particle(p, g, pairs, tp, step, (uint32_t)perm[i]);
+        p = advance_particle(p, g, pairs, tp, step, perm, (size_t)i);
         parts[i] = p;
     }
 }

@@ -66,153 +66,165 @@ __device__ __forceinline__ uint32_t voxel(const GridDev &g, int x, int y, int z)
     return (uint32_t)z * (uint32_t)(g.nx * g.ny) + (uint32_t)(y * g.nx + x);
 }
 
-// Staggered cell of a position: the clamped voxel indices of the three
-// component stencils, and the position in voxel units from the box corner.
-// `key` packs the unclamped floor indices they all derive from, so two
-// positions share a cell exactly when their keys are equal.
-struct Cell {
-    int xO, yO, zO, xM, xP, yM, yP, zM, zP;
-    uint32_t keyO, keyR;
-};
-
-__device__ __forceinline__ Cell cell_of(const GridDev &g, float px, float py, float pz, float3 &gw)
+// Staggered cell of a position.  Every index the three component stencils
+// use derives from k = floor(2 * gi) per axis (gi = the reference's index
+// coordinate): floor(gi) = k >> 1 and floor(gi - 1/2) = (k - 1) >> 1, the
+// latter exact because gi - 1/2 is exact in FP32 wherever the clamp to the
+// grid does not decide the index anyway.  Two positions share a cell when
+// their k, clamped to [-1, 2n], agree: the key packs those.
+__device__ __forceinline__ unsigned long long cell_key(const GridDev &g, float px, float py, float pz, int &kx,
+                                                       int &ky, int &kz)
 {
     const float gix = (g.shift[0] + px) * g.inv_h;
     const float giy = (g.shift[1] + py) * g.inv_h;
     const float giz = (g.shift[2] + pz) * g.inv_h;
-    gw.x = (px - g.mn[0]) * g.inv_h;
-    gw.y = (py - g.mn[1]) * g.inv_h;
-    gw.z = (pz - g.mn[2]) * g.inv_h;
-    Cell c;
-    c.xO = clampi(__float2int_rd(gix), 0, g.nx - 1);
-    c.yO = clampi(__float2int_rd(giy), 0, g.ny - 1);
-    c.zO = clampi(__float2int_rd(giz), 0, g.nz - 1);
-    const int xr = __float2int_rd(gix - 0.5f), yr = __float2int_rd(giy - 0.5f), zr = __float2int_rd(giz - 0.5f);
-    c.xM = clampi(xr, 0, g.nx - 1);
-    c.xP = clampi(xr + 1, 0, g.nx - 1);
-    c.yM = clampi(yr, 0, g.ny - 1);
-    c.yP = clampi(yr + 1, 0, g.ny - 1);
-    c.zM = clampi(zr, 0, g.nz - 1);
-    c.zP = clampi(zr + 1, 0, g.nz - 1);
-    // Clamped indices are in [0, 1023] and xr + 1 in [0, 1024): 10 bits each.
-    c.keyO = (uint32_t)c.xO | ((uint32_t)c.yO << 10) | ((uint32_t)c.zO << 20);
-    c.keyR = (uint32_t)clampi(xr + 1, 0, 1023) | ((uint32_t)clampi(yr + 1, 0, 1023) << 10) |
-             ((uint32_t)clampi(zr + 1, 0, 1023) << 20);
-    return c;
+    kx = clampi(__float2int_rd(2.0f * gix), -1, 2 * g.nx);
+    ky = clampi(__float2int_rd(2.0f * giy), -1, 2 * g.ny);
+    kz = clampi(__float2int_rd(2.0f * giz), -1, 2 * g.nz);
+    return (unsigned long long)(uint32_t)(kx + 1) | ((unsigned long long)(uint32_t)(ky + 1) << 21) |
+           ((unsigned long long)(uint32_t)(kz + 1) << 42);
 }
 
-__device__ __forceinline__ bool same_cell(const Cell &a, const Cell &b)
-{
-    return a.keyO == b.keyO && a.keyR == b.keyR;
-}
-
-// The 24 face samples of a cell as 12 face pairs.
-struct CellSamples {
-    float2 x00, x10, x01, x11;  // x-face pairs at (xO, yM|yP, zM|zP)
-    float2 yM0, yP0, yM1, yP1;  // y-face pairs at (xM|xP, yO, zM|zP)
-    float2 zMM, zMP, zPM, zPP;  // z-face pairs at (xM|xP, yM|yP, zO)
+// The gathered cell: stencil origins as floats and the 24 face samples as 12
+// face pairs, each second sample of a lerp stored as its difference to the
+// first (mixf(x, y, t) = fma(t, y - x, x) then costs one FMA).
+struct CellCache {
+    unsigned long long key;
+    float oxO, oyO, ozO;   // xO, yO, zO
+    float oxM, oyM, ozM;   // xM + 1/2, yM + 1/2, zM + 1/2
+    float2 x00, dx10, x01, dx11;  // x faces at (xO, yM|yP, zM|zP), differences along y
+    float2 yM0, yP0, yM1, yP1;    // y face pairs at (xM|xP, yO, zM|zP), .y = difference along y
+    float2 zMM, dzMP, zPM, dzPP;  // z faces at (xM|xP, yM|yP, zO), differences along y
 };
 
-__device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, const Cell &c,
-                                            CellSamples &s)
+__device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, int kx, int ky,
+                                            int kz, CellCache &c)
 {
+    const int xO = clampi(kx >> 1, 0, g.nx - 1), yO = clampi(ky >> 1, 0, g.ny - 1), zO = clampi(kz >> 1, 0, g.nz - 1);
+    const int xr = (kx - 1) >> 1, yr = (ky - 1) >> 1, zr = (kz - 1) >> 1;
+    const int xM = clampi(xr, 0, g.nx - 1), xP = clampi(xr + 1, 0, g.nx - 1);
+    const int yM = clampi(yr, 0, g.ny - 1), yP = clampi(yr + 1, 0, g.ny - 1);
+    const int zM = clampi(zr, 0, g.nz - 1), zP = clampi(zr + 1, 0, g.nz - 1);
+    c.oxO = (float)xO;
+    c.oyO = (float)yO;
+    c.ozO = (float)zO;
+    c.oxM = (float)xM + 0.5f;
+    c.oyM = (float)yM + 0.5f;
+    c.ozM = (float)zM + 0.5f;
     const uint32_t V = (uint32_t)g.nx * (uint32_t)g.ny * (uint32_t)g.nz;
     const float2 *__restrict__ pxp = pairs;
     const float2 *__restrict__ pyp = pairs + V;
     const float2 *__restrict__ pzp = pairs + 2 * (size_t)V;
-    s.x00 = __ldg(pxp + voxel(g, c.xO, c.yM, c.zM));
-    s.x10 = __ldg(pxp + voxel(g, c.xO, c.yP, c.zM));
-    s.x01 = __ldg(pxp + voxel(g, c.xO, c.yM, c.zP));
-    s.x11 = __ldg(pxp + voxel(g, c.xO, c.yP, c.zP));
-    s.yM0 = __ldg(pyp + voxel(g, c.xM, c.yO, c.zM));
-    s.yP0 = __ldg(pyp + voxel(g, c.xP, c.yO, c.zM));
-    s.yM1 = __ldg(pyp + voxel(g, c.xM, c.yO, c.zP));
-    s.yP1 = __ldg(pyp + voxel(g, c.xP, c.yO, c.zP));
-    s.zMM = __ldg(pzp + voxel(g, c.xM, c.yM, c.zO));
-    s.zMP = __ldg(pzp + voxel(g, c.xM, c.yP, c.zO));
-    s.zPM = __ldg(pzp + voxel(g, c.xP, c.yM, c.zO));
-    s.zPP = __ldg(pzp + voxel(g, c.xP, c.yP, c.zO));
+    const float2 x00 = __ldg(pxp + voxel(g, xO, yM, zM));
+    const float2 x10 = __ldg(pxp + voxel(g, xO, yP, zM));
+    const float2 x01 = __ldg(pxp + voxel(g, xO, yM, zP));
+    const float2 x11 = __ldg(pxp + voxel(g, xO, yP, zP));
+    const float2 yM0 = __ldg(pyp + voxel(g, xM, yO, zM));
+    const float2 yP0 = __ldg(pyp + voxel(g, xP, yO, zM));
+    const float2 yM1 = __ldg(pyp + voxel(g, xM, yO, zP));
+    const float2 yP1 = __ldg(pyp + voxel(g, xP, yO, zP));
+    const float2 zMM = __ldg(pzp + voxel(g, xM, yM, zO));
+    const float2 zMP = __ldg(pzp + voxel(g, xM, yP, zO));
+    const float2 zPM = __ldg(pzp + voxel(g, xP, yM, zO));
+    const float2 zPP = __ldg(pzp + voxel(g, xP, yP, zO));
+    c.x00 = x00;
+    c.dx10 = make_float2(x10.x - x00.x, x10.y - x00.y);
+    c.x01 = x01;
+    c.dx11 = make_float2(x11.x - x01.x, x11.y - x01.y);
+    c.yM0 = make_float2(yM0.x, yM0.y - yM0.x);
+    c.yP0 = make_float2(yP0.x, yP0.y - yP0.x);
+    c.yM1 = make_float2(yM1.x, yM1.y - yM1.x);
+    c.yP1 = make_float2(yP1.x, yP1.y - yP1.x);
+    c.zMM = zMM;
+    c.dzMP = make_float2(zMP.x - zMM.x, zMP.y - zMM.y);
+    c.zPM = zPM;
+    c.dzPP = make_float2(zPP.x - zPM.x, zPP.y - zPM.y);
 }
 
-__device__ __forceinline__ float3 interpolate(const Cell &c, const CellSamples &s, const float3 &gw)
+__device__ __forceinline__ float3 interpolate(const CellCache &c, const float3 &gw)
 {
     float3 v;
     {  // x: faces (xO | xO+1, yM | yP, zM | zP)
-        const float tx = gw.x - (float)c.xO, ty = gw.y - ((float)c.yM + 0.5f), tz = gw.z - ((float)c.zM + 0.5f);
-        const float a = mixf(s.x00.x, s.x10.x, ty);
-        const float b = mixf(s.x00.y, s.x10.y, ty);
-        const float cc = mixf(s.x01.x, s.x11.x, ty);
-        const float d = mixf(s.x01.y, s.x11.y, ty);
+        const float tx = gw.x - c.oxO, ty = gw.y - c.oyM, tz = gw.z - c.ozM;
+        const float a = fmaf(ty, c.dx10.x, c.x00.x);
+        const float b = fmaf(ty, c.dx10.y, c.x00.y);
+        const float cc = fmaf(ty, c.dx11.x, c.x01.x);
+        const float d = fmaf(ty, c.dx11.y, c.x01.y);
         v.x = mixf(mixf(a, b, tx), mixf(cc, d, tx), tz);
     }
     {  // y: faces (xM | xP, yO | yO+1, zM | zP)
-        const float tx = gw.x - ((float)c.xM + 0.5f), ty = gw.y - (float)c.yO, tz = gw.z - ((float)c.zM + 0.5f);
-        const float a = mixf(s.yM0.x, s.yM0.y, ty);
-        const float b = mixf(s.yP0.x, s.yP0.y, ty);
-        const float cc = mixf(s.yM1.x, s.yM1.y, ty);
-        const float d = mixf(s.yP1.x, s.yP1.y, ty);
+        const float tx = gw.x - c.oxM, ty = gw.y - c.oyO, tz = gw.z - c.ozM;
+        const float a = fmaf(ty, c.yM0.y, c.yM0.x);
+        const float b = fmaf(ty, c.yP0.y, c.yP0.x);
+        const float cc = fmaf(ty, c.yM1.y, c.yM1.x);
+        const float d = fmaf(ty, c.yP1.y, c.yP1.x);
         v.y = mixf(mixf(a, b, tx), mixf(cc, d, tx), tz);
     }
     {  // z: faces (xM | xP, yM | yP, zO | zO+1)
-        const float tx = gw.x - ((float)c.xM + 0.5f), ty = gw.y - ((float)c.yM + 0.5f), tz = gw.z - (float)c.zO;
-        const float a = mixf(s.zMM.x, s.zMP.x, ty);
-        const float b = mixf(s.zPM.x, s.zPP.x, ty);
-        const float cc = mixf(s.zMM.y, s.zMP.y, ty);
-        const float d = mixf(s.zPM.y, s.zPP.y, ty);
+        const float tx = gw.x - c.oxM, ty = gw.y - c.oyM, tz = gw.z - c.ozO;
+        const float a = fmaf(ty, c.dzMP.x, c.zMM.x);
+        const float b = fmaf(ty, c.dzPP.x, c.zPM.x);
+        const float cc = fmaf(ty, c.dzMP.y, c.zMM.y);
+        const float d = fmaf(ty, c.dzPP.y, c.zPM.y);
         v.z = mixf(mixf(a, b, tx), mixf(cc, d, tx), tz);
     }
     return v;
 }
 
-// Velocity at a position; `c`/`s` carry the last gathered cell, and the
+// Velocity at a position; `c` carries the last gathered cell, and the
 // samples are loaded again only when the position lies in another cell.
 __device__ __forceinline__ float3 velocity_cached(const GridDev &g, const float2 *__restrict__ pairs, float px,
-                                                  float py, float pz, Cell &c, CellSamples &s, bool &have)
+                                                  float py, float pz, CellCache &c, bool &have)
 {
-    float3 gw;
-    const Cell n = cell_of(g, px, py, pz, gw);
-    if (!have || !same_cell(n, c)) {
-        c = n;
-        gather_cell(g, pairs, c, s);
+    int kx, ky, kz;
+    const unsigned long long key = cell_key(g, px, py, pz, kx, ky, kz);
+    if (!have || key != c.key) {
+        c.key = key;
+        gather_cell(g, pairs, kx, ky, kz, c);
         have = true;
     }
-    return interpolate(c, s, gw);
+    float3 gw;
+    gw.x = (px - g.mn[0]) * g.inv_h;
+    gw.y = (py - g.mn[1]) * g.inv_h;
+    gw.z = (pz - g.mn[2]) * g.inv_h;
+    return interpolate(c, gw);
 }
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
 // One particle step (psfsolver.cpp:75-224): RK1 or RK4 with the box clamp
 // on every stage, lifetime decrement, and respawn from the counter-based
-// generator keyed by the caller-order index `id` when the lifetime ran out.
-// `step` is the index of the step being taken (0 for the first).
+// generator keyed by the caller-order index `perm[idx]` when the lifetime ran
+// out (read only then).  `step` is the index of the step being taken (0 for
+// the first).
 __device__ __forceinline__ float4 advance_particle(float4 p, const GridDev &g, const float2 *__restrict__ u,
-                                                   const TraceParams &tp, uint64_t step, uint32_t id)
+                                                   const TraceParams &tp, uint64_t step,
+                                                   const int32_t *__restrict__ perm, size_t idx)
 {
     if (p.w > 0.f) {
         const float dt = tp.dt;
-        Cell c;
-        CellSamples cs;
+        CellCache c;
         bool have = false;
         float3 v;
         if (tp.rk4) {
-            const float3 k1 = velocity_cached(g, u, p.x, p.y, p.z, c, cs, have);
+            const float3 k1 = velocity_cached(g, u, p.x, p.y, p.z, c, have);
             float qx = clampf(p.x + 0.5f * dt * k1.x, g.mn[0], g.mx[0]);
             float qy = clampf(p.y + 0.5f * dt * k1.y, g.mn[1], g.mx[1]);
             float qz = clampf(p.z + 0.5f * dt * k1.z, g.mn[2], g.mx[2]);
-            const float3 k2 = velocity_cached(g, u, qx, qy, qz, c, cs, have);
+            const float3 k2 = velocity_cached(g, u, qx, qy, qz, c, have);
             qx = clampf(p.x + 0.5f * dt * k2.x, g.mn[0], g.mx[0]);
             qy = clampf(p.y + 0.5f * dt * k2.y, g.mn[1], g.mx[1]);
             qz = clampf(p.z + 0.5f * dt * k2.z, g.mn[2], g.mx[2]);
-            const float3 k3 = velocity_cached(g, u, qx, qy, qz, c, cs, have);
+            const float3 k3 = velocity_cached(g, u, qx, qy, qz, c, have);
             qx = clampf(p.x + dt * k3.x, g.mn[0], g.mx[0]);
             qy = clampf(p.y + dt * k3.y, g.mn[1], g.mx[1]);
             qz = clampf(p.z + dt * k3.z, g.mn[2], g.mx[2]);
-            const float3 k4 = velocity_cached(g, u, qx, qy, qz, c, cs, have);
+            const float3 k4 = velocity_cached(g, u, qx, qy, qz, c, have);
             v.x = (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x) / 6.f;
             v.y = (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y) / 6.f;
             v.z = (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z) / 6.f;
         } else {
-            v = velocity_cached(g, u, p.x, p.y, p.z, c, cs, have);
+            v = velocity_cached(g, u, p.x, p.y, p.z, c, have);
         }
         p.x = clampf(p.x + dt * v.x, g.mn[0], g.mx[0]);
         p.y = clampf(p.y + dt * v.y, g.mn[1], g.mx[1]);
@@ -222,6 +234,7 @@ __device__ __forceinline__ float4 advance_particle(float4 p, const GridDev &g, c
         // psfsolver.cpp:217-222 with the counter-based generator.
         // Particles are stored in cell order; the generator is keyed by the
         // caller's particle index so respawns do not depend on that order.
+        const uint32_t id = (uint32_t)perm[idx];
         const uint32_t r1 = respawn_hash(tp.seed, step, id, 1) % 1024u;
         const uint32_t r2 = respawn_hash(tp.seed, step, id, 2) % 1024u;
         const uint32_t r3 = respawn_hash(tp.seed, step, id, 3) % 1024u;

@@ -1,0 +1,25 @@
+// TMA-staged step kernels of the single-instance (FP32 basis) path.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "psf_internal.h"
+
+namespace psf {
+
+// Tensor maps of C ([k][a][j], tiles of 32 rows x 64 columns) and Phi^T
+// ([i][f], tiles of 64 faces x 64 modes), FP32, no swizzle.
+int make_plain_tma_maps(const PlainDev &d, CUtensorMap *tmC, CUtensorMap *tmP);
+// Row chunks per mode of the contraction (dwpart holds N x this many partials).
+int contract_tma_row_chunks(int N);
+int contract_tma_smem_bytes(int N);
+int reconstruct_tma_smem_bytes(int N);
+int launch_contract_tma(const PlainDev &d, const CUtensorMap &tmC, int grid, int *err, cudaStream_t st);
+int launch_reconstruct_tma(const PlainDev &d, const CUtensorMap &tmP, int grid, int *err, cudaStream_t st);
+
+// FP32 tiled tensor map without swizzle (zero fill outside the tensor).
+int encode_tensor_map_f32(CUtensorMap *map, void *base, int rank, const uint64_t *dims, const uint64_t *strides_bytes,
+                          const uint32_t *box);
+
+}  // namespace psf
