@@ -88,9 +88,7 @@ L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) per launch from one ncu capture of each kernel on
 # the named workload (profiles/step_kernels_sphere32_n128_p262144_rk4.md).
 NCU_TRAFFIC = {
-    ("sphere32_n128_p262144_rk4", "contract_state"): 8410880,
-    ("sphere32_n128_p262144_rk4", "reconstruct"): 45458432 + 1024,
-    ("sphere32_n128_p262144_rk4", "trace"): 4623104,
+    ("sphere32_n128_p262144_rk4", "trace"): 5003520,
 }
 
 
@@ -181,10 +179,8 @@ def kernel_bytes(b, P, kind):
     N = b.n_modes
     Np = (N + 3) // 4 * 4
     Fa = b.n_active
-    if kind == "contract_state":
-        return 4 * N * N * Np + 8 * N * 3
-    if kind == "reconstruct":
-        return 4 * N * ((Fa + 3) // 4 * 4) + 4 * Fa + 4 * Fa + 8 * Fa + 8 * N
+    if kind == "coeff":  # C and Phi read once, partials, face ids and slots read, u and pairs written
+        return 4 * N * N * Np + 8 * N * 3 + 4 * N * ((Fa + 3) // 4 * 4) + 4 * Fa + 4 * Fa + 8 * Fa + 8 * N
     return 32 * P  # trace: read + write float4 per particle
 
 
@@ -260,7 +256,7 @@ def run_ours(args, rank, world, local_rank):
 
     # Kernel breakdown: each kernel between its own events, L2 flushed before each step.
     M = min(K, 64)
-    names = ["contract_state", "reconstruct", "trace"][: ctx.kernels_per_step()]
+    names = ["coeff", "trace"][: ctx.kernels_per_step()]
     acc = np.zeros(len(names))
     for _ in range(M):
         with torch.cuda.stream(stream):

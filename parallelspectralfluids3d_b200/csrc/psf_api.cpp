@@ -155,6 +155,7 @@ struct psf_ctx {
     // TMA kernels report into.
     CUtensorMap tmC{}, tmP{};
     int *err = nullptr;
+    unsigned int *grid_bar = nullptr;
     std::vector<void *> allocs;
 
     ~psf_ctx()
@@ -221,16 +222,11 @@ static int apply_params(psf_ctx *c, const psf_params &p)
     return PSF_OK;
 }
 
-// The coefficient kernels of one step: TMA-staged contraction + state update,
-// then reconstruction.
+// The coefficient half of one step: contraction, state update and
+// reconstruction in one cooperative TMA-staged launch.
 static int launch_coeff(psf_ctx *c, cudaStream_t st)
 {
-    return psf::launch_contract_tma(c->d, c->tmC, c->num_sms, c->err, st);
-}
-
-static int launch_recon(psf_ctx *c, cudaStream_t st)
-{
-    return psf::launch_reconstruct_tma(c->d, c->tmP, c->num_sms, c->err, st);
+    return psf::launch_coeff_tma(c->d, c->tmC, c->tmP, c->num_sms, c->grid_bar, c->err, st);
 }
 
 // Synchronise the context's stream and report a bounded device wait that gave up.
@@ -250,7 +246,6 @@ static int build_graph(psf_ctx *c)
     if (c->exec) return PSF_OK;
     PSF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = launch_coeff(c, c->stream);
-    if (rc == PSF_OK) rc = launch_recon(c, c->stream);
     if (rc == PSF_OK) rc = psf::launch_trace(c->d, c->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
@@ -366,7 +361,7 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phiT, hP.size())) ||
             (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&d.w, (size_t)N)) ||
             (rc = c->alloc(&d.dwpart, (size_t)N * std::max(d.S, psf::contract_tma_row_chunks(N)))) ||
-            (rc = c->alloc(&lam, (size_t)N)) || (rc = c->alloc(&c->err, 1)) ||
+            (rc = c->alloc(&lam, (size_t)N)) || (rc = c->alloc(&c->err, 1)) || (rc = c->alloc(&c->grid_bar, 1)) ||
             (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
             (rc = c->alloc(&d.step_ctr, 1)) || (rc = c->alloc(&d.u, (size_t)F)))
             return bail(rc);
@@ -549,7 +544,7 @@ int psf_get_stream(psf_ctx *c, void **stream)
 int psf_kernels_per_step(psf_ctx *c, int32_t *count)
 {
     if (!c || !count) return fail(PSF_ERR_INVALID, "null argument");
-    *count = c->d.P > 0 ? 3 : 2;
+    *count = c->d.P > 0 ? 2 : 1;
     return PSF_OK;
 }
 
@@ -557,21 +552,19 @@ int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
 {
     if (!c || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
     if (!c->have_state) return fail(PSF_ERR_STATE, "psf_set_state must be called before stepping");
-    const int nk = c->d.P > 0 ? 3 : 2;
+    const int nk = c->d.P > 0 ? 2 : 1;
     if (n < nk) return fail(PSF_ERR_INVALID, "kernel_ms has fewer slots than kernels per step");
     PSF_CUDA(cudaSetDevice(c->device));
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[3];
     for (int i = 0; i <= nk; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
     int rc = PSF_OK;
     cudaStream_t st = c->stream;
     cudaEventRecord(ev[0], st);
     if (rc == PSF_OK) rc = launch_coeff(c, st);
     cudaEventRecord(ev[1], st);
-    if (rc == PSF_OK) rc = launch_recon(c, st);
-    cudaEventRecord(ev[2], st);
-    if (rc == PSF_OK && nk == 3) {
+    if (rc == PSF_OK && nk == 2) {
         rc = psf::launch_trace(c->d, st);
-        cudaEventRecord(ev[3], st);
+        cudaEventRecord(ev[2], st);
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");

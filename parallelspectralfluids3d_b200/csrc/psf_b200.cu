@@ -2,21 +2,15 @@
 // include/psf_b200.h for single-instance contexts.
 //
 // One step (the reference's PSFSolver::integrate, Solver/SolverImpl/
-// psfsolver.cpp:21-234) is three kernels, captured once into a CUDA graph:
+// psfsolver.cpp:21-234) is two kernels, captured once into a CUDA graph: the
+// coefficient half (contraction, FP64 state update, reconstruction) in
+// psf_plain_tma.cu, then
 //
-//   1. psf_contract_state  dw_k = sum_a w_a sum_j C[k][a][j] w_j over an FP32
-//      C streamed with 128-bit loads, FP64 accumulation; the last CTA to
-//      finish (atomic ticket, no spinning) applies the FP64 state update:
-//      Euler step, energy renormalisation, viscous decay, forcing.
-//      (replaces simulation.cl:207-311 and :356-394, five OpenCL kernels)
-//   2. psf_reconstruct     u = Phi w with Phi stored mode-major (faces
-//      contiguous, the tracer's face signs folded in), so every warp streams
-//      512 contiguous bytes per mode; scatter to the reference face numbering
-//      and to the per-voxel face pairs.
-//      (replaces simulation.cl:313-354)
-//   3. psf_trace           one thread per particle, trilinear staggered
-//      interpolation from the signed face field, RK1 or RK4, box clamp,
-//      lifetime and respawn.  (replaces simulation.cl:33-205)
+//   psf_trace   one thread per particle, trilinear staggered interpolation
+//               from the signed face field, RK1 or RK4, box clamp, lifetime
+//               and respawn.  (replaces simulation.cl:33-205)
+//
+// This file also holds the particle ordering kernels and the error helpers.
 
 #include <cuda_runtime.h>
 
@@ -47,150 +41,6 @@ int cuda_fail(cudaError_t e, const char *what)
 {
     return fail(e == cudaErrorMemoryAllocation ? PSF_ERR_NOMEM : PSF_ERR_CUDA,
                 std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-// ------------------------------------------------------- 1. contraction
-// Block b handles mode k = b / S and row slice s = b % S of C_k.  Lane l of a
-// warp owns columns [4l + 128c, 4l + 128c + 4) for c < CH, with w_j in
-// registers; warps walk rows a.  Each lane accumulates
-// sum_a w_a * (C[k][a][j..j+3] . w[j..j+3]) in FP64, so no per-row reduction
-// is needed; one block reduction at the end.
-template <int CH>
-__global__ void __launch_bounds__(256) psf_contract_state(const float *__restrict__ C, int N, int Np, int S,
-                                                          double *__restrict__ w, double *__restrict__ dwpart,
-                                                          const double *__restrict__ lam,
-                                                          const double *__restrict__ force, StateParams sp,
-                                                          unsigned int *__restrict__ ticket,
-                                                          unsigned long long *__restrict__ step_ctr)
-{
-    __shared__ double red[8];
-    __shared__ int is_last;
-    __shared__ double wnew[PSF_MAX_MODES];
-
-    const int k = blockIdx.x / S;
-    const int s = blockIdx.x - k * S;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-    float wj[CH][4];
-#pragma unroll
-    for (int c = 0; c < CH; ++c) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int col = c * 128 + lane * 4 + q;
-            wj[c][q] = col < N ? (float)w[col] : 0.f;
-        }
-    }
-    const int rows = (N + S - 1) / S;
-    const int a0 = s * rows;
-    const int a1 = min(N, a0 + rows);
-    const float *Ck = C + (size_t)k * N * Np;
-    double acc = 0.0;
-#pragma unroll 4
-    for (int a = a0 + warp; a < a1; a += 8) {
-        const float4 *row = reinterpret_cast<const float4 *>(Ck + (size_t)a * Np);
-        float part = 0.f;
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            if (c * 128 + lane * 4 < Np) {
-                const float4 v = __ldg(row + c * 32 + lane);
-                part = fmaf(v.x, wj[c][0], part);
-                part = fmaf(v.y, wj[c][1], part);
-                part = fmaf(v.z, wj[c][2], part);
-                part = fmaf(v.w, wj[c][3], part);
-            }
-        }
-        acc = fma(w[a], (double)part, acc);
-    }
-    const double tot = block_sum_256(acc, red);
-    if (threadIdx.x == 0) {
-        dwpart[blockIdx.x] = tot;
-        __threadfence();
-        const unsigned int prev = atomicAdd(ticket, 1u);
-        is_last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!is_last) return;
-    __threadfence();
-
-    // Last block: FP64 state update in the reference's order
-    // (psfsolver.cpp:37-59).
-    double e1 = 0.0, e2 = 0.0;
-    for (int i = threadIdx.x; i < N; i += 256) {
-        const double wi = w[i];
-        double dw = 0.0;
-        for (int q = 0; q < S; ++q) dw += __ldcg(dwpart + i * S + q);
-        const double w1 = wi + sp.dt * dw;
-        wnew[i] = w1;
-        e1 += wi * wi;
-        e2 += w1 * w1;
-    }
-    e1 = block_sum_256(e1, red);
-    e2 = block_sum_256(e2, red);
-    const double scale = (sp.flags & PSF_FLAG_RENORM) ? sqrt(e1 / e2) : 1.0;
-    for (int i = threadIdx.x; i < N; i += 256) {
-        double v = wnew[i] * scale;
-        v *= exp(sp.visc_signed * lam[i] * sp.dt);
-        if (sp.flags & PSF_FLAG_FORCING) v += sp.dt * force[i];
-        w[i] = v;
-    }
-    if (threadIdx.x == 0) {
-        *ticket = 0u;
-        *step_ctr += 1ull;
-    }
-}
-
-// ---------------------------------------------------- 2. reconstruction
-// 256 threads = 8 warps x 32 lanes; a block covers 128 consecutive active
-// faces (4 per lane, one float4 per mode); warp g sums modes i = g (mod 8).
-__global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__ phiT, long long ldp,
-                                                       const int32_t *__restrict__ faces, long long n_active,
-                                                       int N, const double *__restrict__ w, float *__restrict__ u,
-                                                       float *__restrict__ pairs,
-                                                       const int32_t *__restrict__ pair_dst)
-{
-    __shared__ float wsm[PSF_MAX_MODES];
-    __shared__ float4 red[8][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < N; i += 256) wsm[i] = (float)w[i];
-    __syncthreads();
-    const long long f0 = (long long)blockIdx.x * 128 + lane * 4;
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (f0 < ldp) {
-        const float *base = phiT + f0;
-#pragma unroll 8
-        for (int i = warp; i < N; i += 8) {
-            const float4 v = __ldcs(reinterpret_cast<const float4 *>(base + (size_t)i * ldp));
-            const float wi = wsm[i];
-            acc.x = fmaf(v.x, wi, acc.x);
-            acc.y = fmaf(v.y, wi, acc.y);
-            acc.z = fmaf(v.z, wi, acc.z);
-            acc.w = fmaf(v.w, wi, acc.w);
-        }
-    }
-    red[warp][lane] = acc;
-    __syncthreads();
-    if (warp == 0) {
-        float4 t = red[0][lane];
-#pragma unroll
-        for (int g = 1; g < 8; ++g) {
-            const float4 r = red[g][lane];
-            t.x += r.x;
-            t.y += r.y;
-            t.z += r.z;
-            t.w += r.w;
-        }
-        const float vals[4] = {t.x, t.y, t.z, t.w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const long long r = f0 + q;
-            if (r < n_active) {
-                u[faces[r]] = vals[q];
-                const int32_t d0 = pair_dst[2 * r], d1 = pair_dst[2 * r + 1];
-                if (d0 >= 0) pairs[d0] = vals[q];
-                if (d1 >= 0) pairs[d1] = vals[q];
-            }
-        }
-    }
 }
 
 // Persistent grid (a whole number of resident blocks per SM) striding over
@@ -269,41 +119,6 @@ int launch_unorder_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t
 }
 
 // ------------------------------------------------------------- launchers
-int launch_contract_state(const PlainDev &d, cudaStream_t st)
-{
-    const int CH = (d.Np + 127) / 128;
-    const dim3 grid(d.N * d.S), block(256);
-#define PSF_CASE(n)                                                                                   \
-    case n:                                                                                           \
-        psf_contract_state<n><<<grid, block, 0, st>>>(d.C, d.N, d.Np, d.S, d.w, d.dwpart, d.lam,     \
-                                                      d.force, d.sp, d.ticket, d.step_ctr);          \
-        break;
-    switch (CH) {
-        PSF_CASE(1)
-        PSF_CASE(2)
-        PSF_CASE(3)
-        PSF_CASE(4)
-        PSF_CASE(5)
-        PSF_CASE(6)
-        PSF_CASE(7)
-        PSF_CASE(8)
-    default:
-        return fail(PSF_ERR_UNSUPPORTED, "mode count above the supported maximum");
-    }
-#undef PSF_CASE
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_contract_state launch");
-}
-
-int launch_reconstruct(const PlainDev &d, cudaStream_t st)
-{
-    const long long blocks = (d.n_active + 127) / 128;
-    psf_reconstruct<<<(unsigned)blocks, 256, 0, st>>>(d.phiT, d.ldp, d.faces, d.n_active, d.N, d.w, d.u,
-                                                      reinterpret_cast<float *>(d.pairs), d.pair_dst);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_reconstruct launch");
-}
-
 int trace_blocks_per_sm()
 {
     int per_sm = 0;

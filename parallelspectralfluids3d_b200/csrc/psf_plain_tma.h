@@ -1,4 +1,5 @@
-// TMA-staged step kernels of the single-instance (FP32 basis) path.
+// Coefficient half of a single-instance step (FP32 basis): one cooperative,
+// TMA-staged kernel for contraction, FP64 state update and reconstruction.
 #pragma once
 
 #include <cuda.h>
@@ -13,10 +14,10 @@ namespace psf {
 int make_plain_tma_maps(const PlainDev &d, CUtensorMap *tmC, CUtensorMap *tmP);
 // Row chunks per mode of the contraction (dwpart holds N x this many partials).
 int contract_tma_row_chunks(int N);
-int contract_tma_smem_bytes(int N);
-int reconstruct_tma_smem_bytes(int N);
-int launch_contract_tma(const PlainDev &d, const CUtensorMap &tmC, int grid, int *err, cudaStream_t st);
-int launch_reconstruct_tma(const PlainDev &d, const CUtensorMap &tmP, int grid, int *err, cudaStream_t st);
+int coeff_tma_smem_bytes(int N);
+// One launch per step: `grid_bar` is zeroed on `st` first; one CTA per SM.
+int launch_coeff_tma(const PlainDev &d, const CUtensorMap &tmC, const CUtensorMap &tmP, int num_sms,
+                     unsigned int *grid_bar, int *err, cudaStream_t st);
 
 // FP32 tiled tensor map without swizzle (zero fill outside the tensor).
 int encode_tensor_map_f32(CUtensorMap *map, void *base, int rank, const uint64_t *dims, const uint64_t *strides_bytes,
