@@ -340,7 +340,7 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     d.Np = (int)round_up(N, 4);
     d.S = std::max(1, std::min(N, (2 * c->num_sms + N - 1) / N));
     d.n_active = b->n_active;
-    d.ldp = round_up(b->n_active, 4);
+    d.ldp = round_up(b->n_active, 64);  // whole 64-face tiles
     d.n_faces = F;
     d.P = 0;
 
@@ -349,11 +349,14 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         std::vector<float> hC((size_t)N * N * d.Np, 0.f);
         for (int64_t ka = 0; ka < (int64_t)N * N; ++ka)
             for (int j = 0; j < N; ++j) hC[(size_t)ka * d.Np + j] = (float)b->advection[(size_t)ka * N + j];
-        // Phi mode-major with the tracer's face signs folded in.
+        // Phi as tiles of 64 faces, each tile mode-major ([tile][i][face in tile]),
+        // so one tile's modes are contiguous in memory; the tracer's face signs
+        // are folded in.
         std::vector<float> hP((size_t)N * d.ldp, 0.f);
         for (int64_t r = 0; r < b->n_active; ++r) {
             const float s = (float)c->sigma[(size_t)b->active_faces[r]];
-            for (int i = 0; i < N; ++i) hP[(size_t)i * d.ldp + r] = s * (float)b->phi[(size_t)r * N + i];
+            const size_t base = (size_t)(r / 64) * N * 64 + (size_t)(r % 64);
+            for (int i = 0; i < N; ++i) hP[base + (size_t)i * 64] = s * (float)b->phi[(size_t)r * N + i];
         }
         float *C = nullptr, *phiT = nullptr;
         int32_t *faces = nullptr;

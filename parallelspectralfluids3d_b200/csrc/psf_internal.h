@@ -44,7 +44,7 @@ struct PlainDev {
     int N, Np, S;
     long long n_active, ldp, n_faces, P;
     const float *C;      // [N][N][Np]
-    const float *phiT;   // [N][ldp], signed, mode-major
+    const float *phiT;   // [ldp / 64][N][64]: 64-face tiles, each mode-major; signed
     const int32_t *faces;
     double *w, *dwpart;
     const double *lam, *force;

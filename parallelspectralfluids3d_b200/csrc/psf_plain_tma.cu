@@ -8,7 +8,8 @@
 //   3. every CTA applies the FP64 state update itself, from the partials and
 //      its own shared-memory copy of w^n, in the reference's order
 //      (psfsolver.cpp:37-59); CTA 0 publishes w^{n+1};
-//   4. reconstruction u = Phi w^{n+1}: tiles of 64 faces x 64 modes of Phi^T,
+//   4. reconstruction u = Phi w^{n+1}: tiles of 64 faces x 64 modes of Phi
+//      (stored tile by tile, so each copy is 16 KB of contiguous memory),
 //      summed in FP32 and written to the reference face numbering and to the
 //      per-voxel face-pair field the tracer reads.
 //   (replaces simulation.cl:207-394: advection_reduce_x/y, energy,
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(THREADS, 1) psf_coeff_tma(const __grid_constan
                         tma_load_3d(dst, &tmC, &full[q.stage], ks * CT_COLS, rc * CT_ROWS, k);
                     } else {
                         mbar_arrive_expect_tx(&full[q.stage], RT_BYTES);
-                        tma_load_2d(dst, &tmP, &full[q.stage], t * RT_FACES, ks * RT_MODES);
+                        tma_load_3d(dst, &tmP, &full[q.stage], 0, ks * RT_MODES, t);
                     }
                     issued[q.stage] = true;
                     last_parity[q.stage] = q.phase;
@@ -324,11 +325,12 @@ int make_plain_tma_maps(const PlainDev &d, CUtensorMap *tmC, CUtensorMap *tmP)
     const uint32_t bc[3] = {CT_COLS, CT_ROWS, 1};
     int rc = encode_tensor_map_f32(tmC, const_cast<float *>(d.C), 3, dc, sc, bc);
     if (rc != PSF_OK) return rc;
-    // Phi^T: [i][f] FP32, f padded to ldp (a multiple of 4).
-    const uint64_t dp[2] = {(uint64_t)d.ldp, (uint64_t)d.N};
-    const uint64_t sp[1] = {(uint64_t)d.ldp * 4};
-    const uint32_t bp[2] = {RT_FACES, RT_MODES};
-    return encode_tensor_map_f32(tmP, const_cast<float *>(d.phiT), 2, dp, sp, bp);
+    // Phi: [tile][i][64 faces] FP32 (ldp = whole tiles); a box is 64 modes of one
+    // tile, 16 KB of contiguous memory.
+    const uint64_t dp[3] = {(uint64_t)RT_FACES, (uint64_t)d.N, (uint64_t)(d.ldp / RT_FACES)};
+    const uint64_t sp[2] = {(uint64_t)RT_FACES * 4, (uint64_t)d.N * RT_FACES * 4};
+    const uint32_t bp[3] = {RT_FACES, RT_MODES, 1};
+    return encode_tensor_map_f32(tmP, const_cast<float *>(d.phiT), 3, dp, sp, bp);
 }
 
 int launch_coeff_tma(const PlainDev &d, const CUtensorMap &tmC, const CUtensorMap &tmP, int num_sms,

@@ -9,8 +9,8 @@
 
 namespace psf {
 
-// Tensor maps of C ([k][a][j], tiles of 32 rows x 64 columns) and Phi^T
-// ([i][f], tiles of 64 faces x 64 modes), FP32, no swizzle.
+// Tensor maps of C ([k][a][j], tiles of 32 rows x 64 columns) and Phi
+// ([tile][i][64 faces], boxes of 64 modes of one tile), FP32, no swizzle.
 int make_plain_tma_maps(const PlainDev &d, CUtensorMap *tmC, CUtensorMap *tmP);
 // Row chunks per mode of the contraction (dwpart holds N x this many partials).
 int contract_tma_row_chunks(int N);
