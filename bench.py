@@ -179,8 +179,10 @@ def kernel_bytes(b, P, kind):
     N = b.n_modes
     Np = (N + 3) // 4 * 4
     Fa = b.n_active
-    if kind == "coeff":  # C and Phi read once, partials, face ids and slots read, u and pairs written
-        return 4 * N * N * Np + 8 * N * 3 + 4 * N * ((Fa + 3) // 4 * 4) + 4 * Fa + 4 * Fa + 8 * Fa + 8 * N
+    if kind == "contract_state":
+        return 4 * N * N * Np + 8 * N * 3
+    if kind == "reconstruct":  # Phi read once, face ids and pair slots read, u and pairs written
+        return 4 * N * Fa + 4 * Fa + 4 * Fa + 8 * Fa + 8 * N
     return 32 * P  # trace: read + write float4 per particle
 
 
@@ -256,7 +258,7 @@ def run_ours(args, rank, world, local_rank):
 
     # Kernel breakdown: each kernel between its own events, L2 flushed before each step.
     M = min(K, 64)
-    names = ["coeff", "trace"][: ctx.kernels_per_step()]
+    names = ["contract_state", "reconstruct", "trace"][: ctx.kernels_per_step()]
     acc = np.zeros(len(names))
     for _ in range(M):
         with torch.cuda.stream(stream):

@@ -152,8 +152,8 @@ int psf_kernels_per_step(psf_ctx *ctx, int32_t *count);
 /*
  * Run one step with each kernel launched on its own between CUDA events and
  * return the device time of every kernel in milliseconds, in launch order
- * (contraction + state update + reconstruction in one launch, then tracing
- * when the context holds particles); `n` is the capacity of `kernel_ms`.  Blocks until the step is done.  This is the per-phase
+ * (contraction + state update, reconstruction, tracing); `n` is the capacity
+ * of `kernel_ms`.  Blocks until the step is done.  This is the per-phase
  * timing of the reference's benchmark mode (t_advect_ms, t_particles_ms;
  * Solver/abstractsolver.cpp:252-302, psfsolver.cpp:62-67, 225-231).
  */

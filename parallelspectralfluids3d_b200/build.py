@@ -17,7 +17,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpsf_b200.so")
 TOOL = os.path.join(PKG, "psf_run")
 
-CU_SOURCES = ["psf_b200.cu", "psf_plain_tma.cu", "psf_batch.cu", "psf_noalloc.cu", "psf_voxel.cu", "psf_volume.cu"]
+CU_SOURCES = ["psf_b200.cu", "psf_batch.cu", "psf_noalloc.cu", "psf_voxel.cu", "psf_volume.cu"]
 CPP_SOURCES = ["psf_api.cpp", "psf_batch_api.cpp", "abstractsolver.cpp", "psfsolvercuda.cpp",
                "basis_file.cpp", "psf_engine.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -17,7 +17,6 @@
 
 #include "psf_b200.h"
 #include "psf_internal.h"
-#include "psf_plain_tma.h"
 
 using psf::fail;
 
@@ -151,11 +150,6 @@ struct psf_ctx {
     psf::PlainDev d{};
     psf::OrderBufs order{};
     int32_t *perm = nullptr;
-    // TMA tensor maps of C and Phi^T, and the word the bounded waits of the
-    // TMA kernels report into.
-    CUtensorMap tmC{}, tmP{};
-    int *err = nullptr;
-    unsigned int *grid_bar = nullptr;
     std::vector<void *> allocs;
 
     ~psf_ctx()
@@ -222,22 +216,10 @@ static int apply_params(psf_ctx *c, const psf_params &p)
     return PSF_OK;
 }
 
-// The coefficient half of one step: contraction, state update and
-// reconstruction in one cooperative TMA-staged launch.
-static int launch_coeff(psf_ctx *c, cudaStream_t st)
-{
-    return psf::launch_coeff_tma(c->d, c->tmC, c->tmP, c->num_sms, c->grid_bar, c->err, st);
-}
-
-// Synchronise the context's stream and report a bounded device wait that gave up.
-static int sync_checked(psf_ctx *c)
+// Synchronise the context's stream.
+static int sync_stream(psf_ctx *c)
 {
     PSF_CUDA(cudaStreamSynchronize(c->stream));
-    int code = 0;
-    PSF_CUDA(cudaMemcpy(&code, c->err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (code != 0)
-        return fail(PSF_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(code) +
-                                         "); destroy the context");
     return PSF_OK;
 }
 
@@ -245,7 +227,8 @@ static int build_graph(psf_ctx *c)
 {
     if (c->exec) return PSF_OK;
     PSF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_coeff(c, c->stream);
+    int rc = psf::launch_contract_state(c->d, c->stream);
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->d, c->stream);
     if (rc == PSF_OK) rc = psf::launch_trace(c->d, c->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
@@ -363,8 +346,7 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         double *lam = nullptr, *force = nullptr;
         if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phiT, hP.size())) ||
             (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&d.w, (size_t)N)) ||
-            (rc = c->alloc(&d.dwpart, (size_t)N * std::max(d.S, psf::contract_tma_row_chunks(N)))) ||
-            (rc = c->alloc(&lam, (size_t)N)) || (rc = c->alloc(&c->err, 1)) || (rc = c->alloc(&c->grid_bar, 1)) ||
+            (rc = c->alloc(&d.dwpart, (size_t)N * d.S)) || (rc = c->alloc(&lam, (size_t)N)) ||
             (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
             (rc = c->alloc(&d.step_ctr, 1)) || (rc = c->alloc(&d.u, (size_t)F)))
             return bail(rc);
@@ -390,10 +372,8 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
             (e = cudaMemcpyAsync(lam, b->eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemsetAsync(force, 0, (size_t)N * 8, st)) || (e = cudaMemsetAsync(d.w, 0, (size_t)N * 8, st)) ||
             (e = cudaMemsetAsync(d.ticket, 0, 4, st)) || (e = cudaMemsetAsync(d.step_ctr, 0, 8, st)) ||
-            (e = cudaMemsetAsync(d.u, 0, (size_t)F * 4, st)) || (e = cudaMemsetAsync(c->err, 0, 4, st)) ||
-            (e = cudaStreamSynchronize(st)))
+            (e = cudaMemsetAsync(d.u, 0, (size_t)F * 4, st)) || (e = cudaStreamSynchronize(st)))
             return bail(psf::cuda_fail(e, "basis upload"));
-        if ((rc = psf::make_plain_tma_maps(d, &c->tmC, &c->tmP)) != PSF_OK) return bail(rc);
     } catch (const std::bad_alloc &) {
         return bail(fail(PSF_ERR_NOMEM, "host staging allocation failed"));
     }
@@ -439,7 +419,7 @@ int psf_get_state(psf_ctx *c, double *w, int32_t n)
     if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
     PSF_CUDA(cudaSetDevice(c->device));
     PSF_CUDA(cudaMemcpyAsync(w, c->d.w, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
-    PSF_CHECK(sync_checked(c));
+    PSF_CHECK(sync_stream(c));
     return PSF_OK;
 }
 
@@ -504,7 +484,7 @@ int psf_get_particles(psf_ctx *c, float *xyzw, int64_t count)
     PSF_CUDA(cudaSetDevice(c->device));
     PSF_CHECK(psf::launch_unorder_particles(c->d, c->order, c->stream));
     PSF_CUDA(cudaMemcpyAsync(xyzw, c->order.staging, (size_t)count * 16, cudaMemcpyDeviceToHost, c->stream));
-    PSF_CHECK(sync_checked(c));
+    PSF_CHECK(sync_stream(c));
     return PSF_OK;
 }
 
@@ -514,7 +494,7 @@ int psf_get_velocity(psf_ctx *c, float *u, int64_t n_faces)
     if (n_faces != c->d.n_faces) return fail(PSF_ERR_INVALID, "n_faces must equal the grid's face count");
     PSF_CUDA(cudaSetDevice(c->device));
     PSF_CUDA(cudaMemcpyAsync(u, c->d.u, (size_t)n_faces * 4, cudaMemcpyDeviceToHost, c->stream));
-    PSF_CHECK(sync_checked(c));
+    PSF_CHECK(sync_stream(c));
     for (int64_t f = 0; f < n_faces; ++f) u[f] *= (float)c->sigma[(size_t)f];
     return PSF_OK;
 }
@@ -534,7 +514,7 @@ int psf_sync(psf_ctx *c)
 {
     if (!c) return fail(PSF_ERR_INVALID, "null context");
     PSF_CUDA(cudaSetDevice(c->device));
-    return sync_checked(c);
+    return sync_stream(c);
 }
 
 int psf_get_stream(psf_ctx *c, void **stream)
@@ -547,7 +527,7 @@ int psf_get_stream(psf_ctx *c, void **stream)
 int psf_kernels_per_step(psf_ctx *c, int32_t *count)
 {
     if (!c || !count) return fail(PSF_ERR_INVALID, "null argument");
-    *count = c->d.P > 0 ? 2 : 1;
+    *count = c->d.P > 0 ? 3 : 2;
     return PSF_OK;
 }
 
@@ -555,23 +535,24 @@ int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
 {
     if (!c || !kernel_ms) return fail(PSF_ERR_INVALID, "null argument");
     if (!c->have_state) return fail(PSF_ERR_STATE, "psf_set_state must be called before stepping");
-    const int nk = c->d.P > 0 ? 2 : 1;
+    const int nk = c->d.P > 0 ? 3 : 2;
     if (n < nk) return fail(PSF_ERR_INVALID, "kernel_ms has fewer slots than kernels per step");
     PSF_CUDA(cudaSetDevice(c->device));
-    cudaEvent_t ev[3];
+    cudaEvent_t ev[4];
     for (int i = 0; i <= nk; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
     int rc = PSF_OK;
     cudaStream_t st = c->stream;
     cudaEventRecord(ev[0], st);
-    if (rc == PSF_OK) rc = launch_coeff(c, st);
+    if (rc == PSF_OK) rc = psf::launch_contract_state(c->d, st);
     cudaEventRecord(ev[1], st);
-    if (rc == PSF_OK && nk == 2) {
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->d, st);
+    cudaEventRecord(ev[2], st);
+    if (rc == PSF_OK && nk == 3) {
         rc = psf::launch_trace(c->d, st);
-        cudaEventRecord(ev[2], st);
+        cudaEventRecord(ev[3], st);
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");
-    if (rc == PSF_OK) rc = sync_checked(c);
     for (int i = 0; rc == PSF_OK && i < nk; ++i) {
         float ms = 0.f;
         e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);

@@ -2,17 +2,22 @@
 // include/psf_b200.h for single-instance contexts.
 //
 // One step (the reference's PSFSolver::integrate, Solver/SolverImpl/
-// psfsolver.cpp:21-234) is two kernels, captured once into a CUDA graph: the
-// coefficient half (contraction, FP64 state update, reconstruction) in
-// psf_plain_tma.cu, then
+// psfsolver.cpp:21-234) is three kernels, captured once into a CUDA graph:
 //
-//   psf_trace   one thread per particle, trilinear staggered interpolation
-//               from the signed face field, RK1 or RK4, box clamp, lifetime
-//               and respawn.  (replaces simulation.cl:33-205)
+//   1. psf_contract_state  dw_k = sum_a w_a sum_j C[k][a][j] w_j over an FP32
+//      C streamed with 128-bit loads, FP64 accumulation; the last CTA to
+//      finish (atomic ticket, no spinning) applies the FP64 state update:
+//      Euler step, energy renormalisation, viscous decay, forcing.
+//      (replaces simulation.cl:207-311 and :356-394, five OpenCL kernels)
+//   2. psf_reconstruct     u = Phi w with Phi stored as contiguous 64-face
+//      tiles (the tracer's face signs folded in); scatter to the reference
+//      face numbering and to the per-voxel face pairs.
+//      (replaces simulation.cl:313-354)
+//   3. psf_trace           one thread per particle, trilinear staggered
+//      interpolation from the signed face field, RK1 or RK4, box clamp,
+//      lifetime and respawn.  (replaces simulation.cl:33-205)
 //
-// This file also holds the particle ordering kernels, the error helpers and
-// psf_contract_state, the staging-free contraction + state update that the
-// allocation-free entry point runs.
+// This file also holds the particle ordering kernels and the error helpers.
 
 #include <cuda_runtime.h>
 
@@ -45,9 +50,7 @@ int cuda_fail(cudaError_t e, const char *what)
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// ------------------------------------------- contraction without staging
-// Contraction + FP64 state update with plain 128-bit loads and no tensor
-// maps; psf_coeff_step_static (psf_noalloc.cu) runs it on caller buffers.
+// ------------------------------------------------------- 1. contraction
 // Block b handles mode k = b / S and row slice s = b % S of C_k.  Lane l of a
 // warp owns columns [4l + 128c, 4l + 128c + 4) for c < CH, with w_j in
 // registers; warps walk rows a.  Each lane accumulates
@@ -137,6 +140,63 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
     }
 }
 
+
+// ------------------------------------------------------ reconstruction
+// 256 threads = 8 warps x 32 lanes; a block covers 128 consecutive active
+// faces (4 per lane, one float4 per mode); warp g sums modes i = g (mod 8).
+// Phi is stored as 64-face tiles, each mode-major ([tile][i][64]), so the
+// block's two tiles are 2 x N x 256 contiguous bytes: lanes 0-15 stream one
+// tile, lanes 16-31 the other.
+__global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__ phiT, long long ldp,
+                                                       const int32_t *__restrict__ faces, long long n_active,
+                                                       int N, const double *__restrict__ w, float *__restrict__ u,
+                                                       float *__restrict__ pairs,
+                                                       const int32_t *__restrict__ pair_dst)
+{
+    __shared__ float wsm[PSF_MAX_MODES];
+    __shared__ float4 red[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < N; i += 256) wsm[i] = (float)w[i];
+    __syncthreads();
+    const long long f0 = (long long)blockIdx.x * 128 + lane * 4;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (f0 < ldp) {
+        const float *base = phiT + (size_t)(f0 >> 6) * N * 64 + (f0 & 63);
+#pragma unroll 8
+        for (int i = warp; i < N; i += 8) {
+            const float4 v = __ldcs(reinterpret_cast<const float4 *>(base + (size_t)i * 64));
+            const float wi = wsm[i];
+            acc.x = fmaf(v.x, wi, acc.x);
+            acc.y = fmaf(v.y, wi, acc.y);
+            acc.z = fmaf(v.z, wi, acc.z);
+            acc.w = fmaf(v.w, wi, acc.w);
+        }
+    }
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        float4 t = red[0][lane];
+#pragma unroll
+        for (int g = 1; g < 8; ++g) {
+            const float4 r = red[g][lane];
+            t.x += r.x;
+            t.y += r.y;
+            t.z += r.z;
+            t.w += r.w;
+        }
+        const float vals[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const long long r = f0 + q;
+            if (r < n_active) {
+                u[faces[r]] = vals[q];
+                const int32_t d0 = pair_dst[2 * r], d1 = pair_dst[2 * r + 1];
+                if (d0 >= 0) pairs[d0] = vals[q];
+                if (d1 >= 0) pairs[d1] = vals[q];
+            }
+        }
+    }
+}
 
 // Persistent grid (a whole number of resident blocks per SM) striding over
 // the particles, which are stored in cell order.
@@ -241,6 +301,15 @@ int launch_contract_state(const PlainDev &d, cudaStream_t st)
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_contract_state launch");
 }
 
+
+int launch_reconstruct(const PlainDev &d, cudaStream_t st)
+{
+    const long long blocks = (d.n_active + 127) / 128;
+    psf_reconstruct<<<(unsigned)blocks, 256, 0, st>>>(d.phiT, d.ldp, d.faces, d.n_active, d.N, d.w, d.u,
+                                                      reinterpret_cast<float *>(d.pairs), d.pair_dst);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_reconstruct launch");
+}
 
 int trace_blocks_per_sm()
 {

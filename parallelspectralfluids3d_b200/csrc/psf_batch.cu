@@ -756,34 +756,6 @@ int encode_tensor_map(CUtensorMap *map, void *base, int rank, const uint64_t *di
     return PSF_OK;
 }
 
-int encode_tensor_map_f32(CUtensorMap *map, void *base, int rank, const uint64_t *dims, const uint64_t *strides_bytes,
-                          const uint32_t *box)
-{
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
-            return fail(PSF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-        fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
-    cuuint64_t d[5];
-    cuuint64_t s[4];
-    cuuint32_t bx[5], es[5];
-    for (int i = 0; i < rank; ++i) {
-        d[i] = dims[i];
-        bx[i] = box[i];
-        es[i] = 1;
-        if (i + 1 < rank) s[i] = strides_bytes[i];
-    }
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, base, d, s, bx, es,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(PSF_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
-    return PSF_OK;
-}
-
 void split_bf16_host(double x, uint16_t *hi, uint16_t *lo)
 {
     const __nv_bfloat16 h = __float2bfloat16_rn((float)x);

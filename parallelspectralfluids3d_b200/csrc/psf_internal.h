@@ -98,6 +98,7 @@ int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 
 int launch_contract_state(const PlainDev &d, cudaStream_t st);
+int launch_reconstruct(const PlainDev &d, cudaStream_t st);
 int launch_trace(const PlainDev &d, cudaStream_t st);
 int trace_blocks_per_sm();
 int sort_particles_temp_bytes(long long P, size_t *bytes);

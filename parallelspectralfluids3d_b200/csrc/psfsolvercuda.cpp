@@ -135,10 +135,10 @@ void PSFSolverCUDA::integrate()
     if (benchmarkFrameNo > maxFramesBenchmark) startBenchmark(false);
     if (isBenchmark) {
         ++benchmarkFrameNo;
-        double ms[2] = {0, 0};
-        check(psf_profile_step(ctx, ms, 2), "psf_profile_step");
-        benchmarkSums[0] += ms[0];  // coefficient update + reconstruction
-        benchmarkSums[1] += ms[1];  // particles (0 without particles)
+        double ms[3] = {0, 0, 0};
+        check(psf_profile_step(ctx, ms, 3), "psf_profile_step");
+        benchmarkSums[0] += ms[0] + ms[1];  // coefficient update + reconstruction
+        benchmarkSums[1] += ms[2];          // particles (0 without particles)
         pullState();
         simTime += 1.0;
         return;
