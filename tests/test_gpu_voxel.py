@@ -31,7 +31,7 @@ MESHES = {
 
 @pytest.mark.parametrize("mode", [voxel.REFERENCE, voxel.GEOMETRIC])
 @pytest.mark.parametrize("name", sorted(MESHES))
-@pytest.mark.parametrize("res", [1 / 32, 0.0173])
+@pytest.mark.parametrize("res", [1 / 32, 1 / 40, 0.0173])
 def test_voxelize_matches_oracle(name, mode, res):
     v, t = MESHES[name]()
     want = VO.voxelize(v, t, res, mode)
