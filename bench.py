@@ -88,7 +88,9 @@ L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) per launch from one ncu capture of each kernel on
 # the named workload (profiles/step_kernels_sphere32_n128_p262144_rk4.md).
 NCU_TRAFFIC = {
-    ("sphere32_n128_p262144_rk4", "trace"): 5003520,
+    ("sphere32_n128_p262144_rk4", "contract_state"): 8410880,
+    ("sphere32_n128_p262144_rk4", "reconstruct"): 46189056,
+    ("sphere32_n128_p262144_rk4", "trace"): 5003776,
 }
 
 
