@@ -1,7 +1,7 @@
 // Minimal dense vector / matrix types for the headless solver interface.
 //
 // The reference's getters return Eigen types (Solver/abstractsolver.h:40-47);
-// Eigen is not part of this build, so these column-major containers stand in
+// Eigen is not a dependency of this library, so these column-major containers stand in
 // with the subset of the interface the solver uses (size, element access,
 // raw data).
 #pragma once

@@ -1,6 +1,6 @@
 """GPU path (through the C ABI) against the FP64 oracle.
 
-Tolerances (BASELINE north star): the FP32 plain path stays within 1e-5
+Tolerances: the FP32 plain path stays within 1e-5
 relative on w after 100 steps and within 1e-4 voxel on particle positions on
 the 16^3 / N = 64 workload; small domains use the same bars.
 """
