@@ -163,3 +163,90 @@ def test_voxelised_mesh_builds_a_domain():
     d = voxel.to_domain(m, dims, res, mn, mx, name="sphere12").build()
     assert d.dims == dims and d.inside.sum() == m.sum()
     assert d.n_voxels == m.size
+
+
+# ------------------------------------------------------------ literal slice map
+def _literal_slice_map(v, t, res):
+    """The reference's slice map, restated literally in Python for small meshes: every covered
+    pixel centre builds the RGBA32UI mask of voxel.frag (bits [0, z) over r, g, b, a, one bit at a
+    time) in the layer of the triangle's last vertex (voxel.geom), XORs it into the texel
+    (GL_XOR logic op, Model.cpp:249-256), and the read-back walks channels and bits with the
+    reference's shifts (Model.cpp:278-441).  Coverage uses the same fixed rules as the oracle."""
+    f32 = np.float32
+    v = np.asarray(v, f32)
+    mn = np.minimum(v.min(0), 0).astype(f32)
+    mx = np.maximum(v.max(0), 0).astype(f32)
+    ext = (mx - mn).astype(f32)
+    W, H, D = (int(np.ceil(f32(ext[a] / f32(res)))) for a in range(3))
+    layers = max(1, int(np.ceil(f32(ext[2] / f32(f32(res) * f32(128))))))
+    ctr_z = f32(mn[2] + f32(f32(0.5) * f32(mx[2] - mn[2])))
+    zo = f32(ext[2] * f32(0.5))
+    tex = np.zeros((layers, H, W, 4), np.uint64)
+
+    def proj(p):
+        xw = f32(f32(f32(p[0] - mn[0]) / ext[0]) * f32(W))
+        yw = f32(f32(f32(p[1] - mn[1]) / ext[1]) * f32(H))
+        top = f32(f32(ctr_z - p[2]) + zo)
+        return int(np.rint(f32(xw * f32(256)))), int(np.rint(f32(yw * f32(256)))), f32(top / f32(res)), \
+            np.floor(f32(top / f32(f32(res) * f32(128))))
+
+    def edge(a, b, px, py):
+        return (b[0] - a[0]) * (py - a[1]) - (b[1] - a[1]) * (px - a[0])
+
+    def owns(dx, dy):
+        return dy < 0 or (dy == 0 and dx > 0)
+
+    for tri in np.asarray(t).reshape(-1, 3):
+        q = [proj(v[i]) for i in tri]
+        area = edge(q[0], q[1], q[2][0], q[2][1])
+        if area == 0:
+            continue
+        A, B, C = (q[0], q[1], q[2]) if area > 0 else (q[0], q[2], q[1])
+        lay, zc = q[2][3], q[2][2]
+        if not (lay >= 0) or lay >= layers:
+            continue
+        zbits = int(zc) if zc > 0 else 0
+        mask = [0, 0, 0, 0]
+        for c in range(4):                      # voxel.frag:25-48
+            for d in range(32):
+                if zbits != 0:
+                    mask[c] |= 1 << d
+                    zbits -= 1
+        for j in range(H):
+            for i in range(W):
+                px, py = i * 256 + 128, j * 256 + 128
+                e0, e1, e2 = edge(B, C, px, py), edge(C, A, px, py), edge(A, B, px, py)
+                if not (e0 > 0 or (e0 == 0 and owns(C[0] - B[0], C[1] - B[1]))):
+                    continue
+                if not (e1 > 0 or (e1 == 0 and owns(A[0] - C[0], A[1] - C[1]))):
+                    continue
+                if not (e2 > 0 or (e2 == 0 and owns(B[0] - A[0], B[1] - A[1]))):
+                    continue
+                for c in range(4):
+                    tex[int(lay), j, i, c] ^= mask[c]
+    inside = np.zeros((D, H, W), np.uint8)
+    for l in range(layers):
+        for y in range(H):
+            for x in range(W):
+                for c in range(4):
+                    word = int(tex[l, y, x, c])
+                    for d in range(32):
+                        z = 128 * l + 32 * c + d
+                        if word & 1 and z < D:
+                            inside[z, y, x] = 1
+                        word >>= 1
+    return inside
+
+
+@pytest.mark.parametrize("case", ["box", "sphere", "layered"])
+def test_oracle_matches_a_literal_slice_map(case):
+    if case == "box":
+        v, t = voxel.box_mesh([-0.4, -0.3, -0.5], [0.3, 0.45, 0.2])
+        res = 0.07
+    elif case == "sphere":
+        v, t = voxel.icosphere(2, 0.4, center=(0.05, -0.02, 0.01))
+        res = 0.06
+    else:  # depth 150: two 128-slice layers
+        v, t = voxel.box_mesh([-0.05, -0.05, -0.75], [0.05, 0.05, 0.0])
+        res = 0.005
+    assert np.array_equal(VO.voxelize(v, t, res, VO.REFERENCE), _literal_slice_map(v, t, res))
