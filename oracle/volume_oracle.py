@@ -7,6 +7,8 @@ Only ``tests/`` and ``bench.py``'s CPU baseline leg use this module.
 
 Parity unpinned: the reference renders through OpenGL, which is unavailable
 here, its histogram shader is missing from its tree, and it ships no images.
+The C restatement is checked against known answers and, pixel by pixel,
+against a line-by-line FP32 replay of volume.frag in Python (tests/test_volume.py).
 """
 
 from __future__ import annotations

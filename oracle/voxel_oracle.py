@@ -8,7 +8,9 @@ Parity unpinned: the reference voxelises through OpenGL, which is unavailable
 here, and ships no voxelised fixtures; the restatement fixes GL's
 implementation-defined rasterisation rules (1/256-pixel snapping, exact edge
 functions, a down-or-right edge ownership rule) and is checked against
-known answers instead (axis-aligned boxes, spheres, watertightness).
+known answers instead (axis-aligned boxes, spheres, watertightness) and
+against a literal Python replay of the shader's bit loops and of the
+read-back loops (tests/test_voxel.py).
 """
 
 from __future__ import annotations
