@@ -179,9 +179,11 @@ int psf_profile_step(psf_ctx *ctx, double *kernel_ms, int32_t n);
  * The kernel's scratch lives in a fixed array of PSF_STATIC_SCRATCH_BYTES in
  * the library's device data, held by every GPU that loads the library until
  * the process exits.  N is limited to PSF_STATIC_MAX_MODES (larger sizes
- * return PSF_ERR_UNSUPPORTED).  The first call on a device looks up that
- * array's device address (cudaGetSymbolAddress) with the device current;
- * make that first call before any stream capture.  The function never calls
+ * return PSF_ERR_UNSUPPORTED).  The first call in each CUDA context (on
+ * each device, and again after cudaDeviceReset or with another context made
+ * current) looks up that array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture: made while `stream` is
+ * capturing, it returns PSF_ERR_STATE and enqueues nothing.  The function never calls
  * cudaMalloc or cudaFree.  All calls share the one array: calls whose
  * kernels may overlap on the GPU (unordered streams or threads) race and
  * corrupt each other's results, so order them on one stream.

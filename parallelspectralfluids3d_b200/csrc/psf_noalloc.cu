@@ -39,33 +39,74 @@ static_assert(kScratchBytes == PSF_STATIC_SCRATCH_BYTES, "header and implementat
 
 // The scratch itself.  Host code may not use this name as a device address:
 // on the host it names a shadow variable, so its address is looked up with
-// cudaGetSymbolAddress once per device (with that device current).
+// cudaGetSymbolAddress once per CUDA context (with that context current).
 static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char *g_scratch_dev[kMaxDevices] = {};
+void *g_scratch_ctx[kMaxDevices] = {};  // the context the address above belongs to
 int g_num_sms[kMaxDevices] = {};
 
+// cuCtxGetCurrent through the runtime's driver entry point (no link against
+// libcuda).  The module holding the scratch array is loaded once per context,
+// so a device address is valid only while the context it was resolved in is
+// current: after cudaDeviceReset, or with another context made current on
+// the same GPU, the array lives at a new address.
+using CtxGetCurrentFn = int (*)(void **);
+
+int current_context(void **ctx)
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    });
+    *ctx = nullptr;
+    if (!fn) return psf::fail(PSF_ERR_CUDA, "cuCtxGetCurrent is not available from the CUDA driver");
+    if (fn(ctx) != 0) return psf::fail(PSF_ERR_CUDA, "cuCtxGetCurrent failed");
+    return PSF_OK;
+}
+
 // Resolve the device address of the scratch array and the SM count for the
-// current device; done once per device, on the first call there.
-int setup_current_device(int *device_out, unsigned char **scratch, int *num_sms)
+// current device.  Done on the first call in each context; a lookup needs
+// the module loaded, which a stream capture cannot do, so a first call made
+// while `stream` is capturing is refused with PSF_ERR_STATE.
+int setup_current_device(cudaStream_t stream, int *device_out, unsigned char **scratch, int *num_sms)
 {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return psf::cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices)
         return psf::fail(PSF_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table");
+    void *ctx = nullptr;
+    int rc = current_context(&ctx);
+    if (rc != PSF_OK) return rc;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_dev[dev]) {
+    if (!ctx || !g_scratch_dev[dev] || g_scratch_ctx[dev] != ctx) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        e = cudaStreamIsCapturing(stream, &cs);
+        if (e != cudaSuccess) return psf::cuda_fail(e, "cudaStreamIsCapturing");
+        if (cs != cudaStreamCaptureStatusNone)
+            return psf::fail(PSF_ERR_STATE, "psf_coeff_step_static: the first call in a CUDA context must not be "
+                                            "made during stream capture (it looks up the scratch array)");
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) return psf::cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+        // The lookup made the runtime's context current if none was: record that one.
+        rc = current_context(&ctx);
+        if (rc != PSF_OK) return rc;
+        if (!ctx) return psf::fail(PSF_ERR_CUDA, "no current CUDA context");
         int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return psf::cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
         g_num_sms[dev] = sms;
         g_scratch_dev[dev] = static_cast<unsigned char *>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *device_out = dev;
     *scratch = g_scratch_dev[dev];
@@ -88,7 +129,8 @@ extern "C" int psf_coeff_step_static(const float *advection_f32, int32_t n_modes
 
     int dev = 0, num_sms = 0;
     unsigned char *scratch = nullptr;
-    int rc = setup_current_device(&dev, &scratch, &num_sms);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = setup_current_device(st, &dev, &scratch, &num_sms);
     if (rc != PSF_OK) return rc;
 
     // Same work split as a context's step (psf_create), so the result is the
@@ -113,7 +155,6 @@ extern "C" int psf_coeff_step_static(const float *advection_f32, int32_t n_modes
     d.sp.visc_signed = (params->flags & PSF_FLAG_DECAY_NEG) ? -params->viscosity : params->viscosity;
     d.sp.flags = params->flags;
 
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(d.ticket, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return psf::cuda_fail(e, "clearing the static ticket");
     return psf::launch_contract_state(d, st);

@@ -37,12 +37,20 @@ def _device_inputs(torch, b, w0, forcing):
             torch.from_numpy(np.ascontiguousarray(forcing, dtype=np.float64)).to(dev))
 
 
+@pytest.fixture(params=["box16_n64", "box16_n4", "box12_n160"])
+def static_basis(request, c1_basis, medium_basis):
+    """Mode counts that reach the kernel's one- and two-chunk templates and its
+    smallest and largest row splits (N = 4 splits each mode over 4 blocks)."""
+    return {"box16_n64": lambda: c1_basis, "box16_n4": lambda: c1_basis.truncate(4),
+            "box12_n160": lambda: medium_basis}[request.param]()
+
+
 @pytest.mark.parametrize("flags", [L.PSF_FLAG_RENORM, L.PSF_FLAG_RENORM | L.PSF_FLAG_FORCING])
-def test_static_scratch_step_matches_context_step(c1_basis, flags):
+def test_static_scratch_step_matches_context_step(static_basis, flags):
     import torch
 
     lib = L.load()
-    b = c1_basis
+    b = static_basis
     w0 = initial_coefficients(b.n_modes, 11)
     forcing = np.zeros(b.n_modes)
     forcing[0] = 0.1 / 0.01
