@@ -95,6 +95,12 @@ def load(path: str | None = None):
         raise ImportError(
             f"{path} is missing; build it with `python -m parallelspectralfluids3d_b200.build`"
         )
+    if path == LIB_PATH:
+        from . import build as _build
+
+        if not _build.is_current():
+            raise ImportError(f"{path} was not built from the sources beside it; rebuild it with "
+                              "`python -m parallelspectralfluids3d_b200.build`")
     L = ct.CDLL(path)
     vp = ct.c_void_p
     L.psf_abi_version.restype = ct.c_int
@@ -122,11 +128,12 @@ def load(path: str | None = None):
 
 def _extend(L):
     """Declare the batch, engine, voxeliser and volume entry points."""
-    from . import _lib_batch, _lib_engine, _lib_volume, _lib_voxel
+    from . import _lib_batch, _lib_engine, _lib_pre, _lib_volume, _lib_voxel
 
     _lib_batch.declare(L)
     _lib_engine.declare(L)
     _lib_voxel.declare(L)
+    _lib_pre.declare(L)
     _lib_volume.declare(L)
 
 
