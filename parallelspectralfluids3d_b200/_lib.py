@@ -127,7 +127,7 @@ def load(path: str | None = None):
 
 
 def _extend(L):
-    """Declare the batch, engine, voxeliser and volume entry points."""
+    """Declare the batch, engine, voxeliser, volume and precompute entry points."""
     from . import _lib_batch, _lib_engine, _lib_pre, _lib_volume, _lib_voxel
 
     _lib_batch.declare(L)
