@@ -66,3 +66,69 @@ def test_two_gloo_ranks_take_the_slowest_time():
     for _, mine, rate, both in res:
         assert rate == pytest.approx(2 * 5 / 0.040)
         assert both == [40.0, 1.0]
+
+
+def _serve_rank(rank, world, port, out):
+    """A CPU stand-in for one rank's engine: it serves its round-robin share of a
+    Poisson request stream (each request takes steps x 10 us) and rank 0
+    combines every rank's completions."""
+    import datetime
+    import time
+
+    import numpy as np
+    import torch.distributed as td
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    td.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        rng = np.random.default_rng(7)
+        arrivals = np.cumsum(rng.exponential(1 / 2000.0, 40))
+        reqs = [dict(index=i, t=float(t), steps=int(rng.integers(50, 1001))) for i, t in enumerate(arrivals)]
+        mine = replicas.shard(reqs, rank, world)
+        t0 = time.monotonic()
+        lat, first, last = [], None, None
+        for q in mine:
+            wait = q["t"] - (time.monotonic() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            submit = time.monotonic()
+            time.sleep(q["steps"] * 1e-5)
+            end = time.monotonic()
+            first = submit if first is None else first
+            last = end
+            lat.append(end - submit)
+        rec = {"requests": [q["index"] for q in mine], "latencies": lat, "steps": sum(q["steps"] for q in mine),
+               "first": first, "last": last}
+        recs = replicas.gather_objects(rec)
+        job = replicas.combine_serving(recs)
+        out.put((rank, job, sum(q["steps"] for q in reqs)))
+    finally:
+        td.destroy_process_group()
+
+
+def test_two_gloo_ranks_serve_a_sharded_request_stream():
+    world = 2
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_serve_rank, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [out.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for _, job, total in res:
+        assert job["requests"] == list(range(40))  # every request served once, by one rank
+        assert job["per_rank_completed"] == [20, 20]
+        assert job["instance_steps"] == total
+        assert job["instance_steps_per_s"] == pytest.approx(total / job["span_s"])
+        assert 0 < job["p50_latency_s"] <= job["p99_latency_s"]
+
+
+def test_combine_serving_rejects_a_request_served_twice():
+    recs = [{"requests": [0, 1], "latencies": [0.1, 0.2], "steps": 10, "first": 0.0, "last": 1.0},
+            {"requests": [1], "latencies": [0.1], "steps": 5, "first": 0.5, "last": 2.0}]
+    with pytest.raises(RuntimeError):
+        replicas.combine_serving(recs)
