@@ -82,7 +82,9 @@ def basis_cache_for(name, n):
             return d
     return BIG_BASIS_CACHE
 DEFAULT_WORKLOAD = "sphere32_n128_p262144_rk4"
+REFERENCE_MIN_STEPS = 300
 FORM_WORKLOAD = "sphere32_n128_p262144_rk4_b64"
+MIXED_WORKLOAD = "mixed512_p16384"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 # DRAM bytes (read + write) per launch from one ncu capture of each kernel on
@@ -103,6 +105,14 @@ def make_domain(spec):
     if kind == "channel":
         return channel_domain(n)
     return box_domain(n)
+
+
+def plain_config(name, b, wl, parts, world=1):
+    """The ``config`` object of a plain-workload line (the same for both arms)."""
+    return {"workload": name, "describe": wl["describe"], "n_modes": b.n_modes, "faces_active": b.n_active,
+            "particles": int(parts.shape[0]), "integrator": "rk4" if wl["integrator"] == 4 else "rk1",
+            "dt": wl["dt"], "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
+            "parallelism": f"replicas x{world}"}
 
 
 def load_workload(name, device):
@@ -315,10 +325,7 @@ def run_ours(args, rank, world, local_rank):
         "n_gpus": world, "steps": K, "warmup": max(3, args.warmup), "ms_per_step": round(total_ms / K, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "state_dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "describe": wl["describe"], "n_modes": b.n_modes,
-                   "faces_active": b.n_active, "particles": int(parts.shape[0]),
-                   "integrator": "rk4" if wl["integrator"] == 4 else "rk1", "dt": wl["dt"],
-                   "l2": "flushed before every timed step (256 MB write, then 256 MB read)", "parallelism": f"replicas x{world}"},
+        "config": plain_config(args.workload, b, wl, parts, world),
         "p50_ms": round(float(np.percentile(per_step, 50)), 5),
         "p99_ms": round(float(np.percentile(per_step, 99)), 5),
         "particle_steps_per_s": round(value * parts.shape[0], 1),
@@ -333,6 +340,14 @@ def run_ours(args, rank, world, local_rank):
         form["e2e_speedup_vs_plain"] = round(form["e2e"]["value"] / e2e["value"], 3)
         line["forms"] = {"batched_bf16x2": dict(workload=FORM_WORKLOAD, **form)}
         line["gpu_launches"] += form["gpu_launches"]
+        # The batching form (512 instances of uneven N on three domains): its
+        # bases come from the GPU precompute on this device, and its plain-path
+        # denominator is the single-instance path on a sample of the same instances.
+        t0 = time.perf_counter()
+        mixed = run_batch(args, MIXED_WORKLOAD, local_rank, plain=True)
+        mixed["wall_s"] = round(time.perf_counter() - t0, 1)
+        line["forms"]["batched_mixed512"] = dict(workload=MIXED_WORKLOAD, **mixed)
+        line["gpu_launches"] += mixed["gpu_launches"]
     return line
 
 
@@ -355,9 +370,11 @@ def accuracy_and_cpu(b, wl, w0, parts, force, params, device):
     ref.step(S)
     cpu_s = time.perf_counter() - t0
     rel = float(np.linalg.norm(w_gpu - ref.w) / np.linalg.norm(ref.w))
-    perr = float(np.abs(p_gpu[:, :3] - ref.pos).max() / b.h)
+    d = np.abs(p_gpu[:, :3] - ref.pos).max(axis=1) / b.h
     return {
-        "accuracy": {"steps": S, "rel_err_w_vs_fp64": rel, "max_particle_err_voxels": perr},
+        "accuracy": {"steps": S, "rel_err_w_vs_fp64": rel, "max_particle_err_voxels": float(d.max()),
+                     "p99_particle_err_voxels": float(np.percentile(d, 99)),
+                     "p50_particle_err_voxels": float(np.percentile(d, 50))},
         "cpu_baseline": {"value": round(S / cpu_s, 3), "unit": "instance-steps/s", "cores": O.num_threads(),
                          "kind": "port", "sample": f"full {S}-step run of the workload, FP64, OpenMP"},
     }
@@ -374,7 +391,9 @@ def run_reference(args):
     O.build()
     ref = O.OracleRollout(b, w0, parts, dt=wl["dt"], integrator=wl["integrator"], forcing=force)
     ref.step(max(3, args.warmup))
-    K = args.steps
+    # At least REFERENCE_MIN_STEPS steps (about 2 s on the workload) so that the
+    # rate is not a handful of noisy steps; never more than the full run.
+    K = min(max(args.steps, REFERENCE_MIN_STEPS), wl["full_steps"])
     t0 = time.perf_counter()
     ref.step(K)
     dt = time.perf_counter() - t0
@@ -383,7 +402,7 @@ def run_reference(args):
         "impl": "reference", "metric": "instance-steps/s", "value": round(value, 3), "unit": "instance-steps/s",
         "n_gpus": 1, "steps": K, "warmup": max(3, args.warmup), "ms_per_step": round(1e3 * dt / K, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "describe": wl["describe"]},
+        "config": plain_config(args.workload, b, wl, parts),
         "cpu_baseline": {"value": round(value, 3), "unit": "instance-steps/s", "cores": O.num_threads(),
                          "kind": "port",
                          "sample": f"{K} steps of the full workload (reference does not build: Eigen/glm absent)"},
@@ -415,6 +434,15 @@ def load_batch_workload(name, device):
     for x in insts:
         x["parts"] = initial_particles(bases[x["basis"]], wl["particles"], x["seed_p"])
     return wl, bases, slots, insts
+
+
+def assign_slots(insts, n_bases):
+    """Number each instance's slot within its basis (in order) and count the slots per basis."""
+    counts = [0] * n_bases
+    for x in insts:
+        x["slot"] = counts[x["basis"]]
+        counts[x["basis"]] += 1
+    return [max(1, c) for c in counts]
 
 
 def batch_params(wl, x):
@@ -452,8 +480,12 @@ def batch_kernel_bytes(bases, slots, insts, kind):
     return tot, flops
 
 
-def run_batch(args, name, local_rank, flush=True, check=True, plain=True):
-    """Time a batched workload: device instance-steps/s, kernel roofline, e2e rollouts, FP64 error."""
+def run_batch(args, name, local_rank, flush=True, check=True, plain=True, rank=0, world=1):
+    """Time a batched workload: device instance-steps/s, kernel roofline, e2e rollouts, FP64 error.
+
+    With ``world > 1`` this rank takes its round-robin share of the instances
+    (replicas.shard) and steps them as its own batch.
+    """
     import torch
 
     from parallelspectralfluids3d_b200.batch import Batch
@@ -461,6 +493,10 @@ def run_batch(args, name, local_rank, flush=True, check=True, plain=True):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     wl, bases, slots, insts = load_batch_workload(name, "cuda")
+    n_total = len(insts)
+    if world > 1:
+        insts = replicas.shard(insts, rank, world)
+        slots = assign_slots(insts, len(bases))
     P = wl["particles"]
     t0 = time.perf_counter()
     batch = Batch(bases, slots=slots, max_particles=P, device=local_rank, autotune=True)
@@ -560,7 +596,8 @@ def run_batch(args, name, local_rank, flush=True, check=True, plain=True):
     e2e = {"value": round(B * E / (e2e_ms / 1e3), 2), "unit": "instance-steps/s",
            "h2d_bytes_per_step": int(h2d // E), "d2h_bytes_per_step": int(d2h // E),
            "rollout_steps": E}
-    out = {"value": round(value, 2), "unit": "instance-steps/s", "instances": B, "steps": K,
+    out = {"value": round(value, 2), "unit": "instance-steps/s", "instances": B, "instances_total": n_total,
+           "steps": K,
            "ms_per_step": round(total_ms / K, 5), "p50_ms": round(float(np.percentile(per_step, 50)), 5),
            "p99_ms": round(float(np.percentile(per_step, 99)), 5),
            "particle_steps_per_s": round(value * P, 1), "kernel_ms": kms_step,
@@ -644,22 +681,26 @@ def run_batch_line(args, rank, world, local_rank):
 
     args.batch_steps = args.steps if args.steps else args.batch_steps
     clocks = ClockSampler(local_rank).start()
-    r = run_batch(args, args.workload, local_rank, check=(rank == 0 and world == 1 and not args.no_cpu))
+    r = run_batch(args, args.workload, local_rank, check=(rank == 0 and world == 1 and not args.no_cpu),
+                  plain=(world == 1), rank=rank, world=world)
     clk = clocks.stop()
     total_ms = r["ms_per_step"] * r["steps"]
     e2e_v = r["e2e"]["value"]
     total_ms, inv = replicas.slowest([total_ms, 1.0 / max(e2e_v, 1e-30)], device=torch.device("cuda", local_rank))
     e2e_v = 1.0 / inv
-    value = world * r["instances"] * r["steps"] / (total_ms / 1e3)
-    e2e = dict(r["e2e"], value=round(world * e2e_v, 2))
+    # Whole job: every rank's instances (a round-robin share of the workload)
+    # over the slowest rank's device time.
+    value = r["instances_total"] * r["steps"] / (total_ms / 1e3)
+    e2e = dict(r["e2e"], value=round(e2e_v * r["instances_total"] / r["instances"], 2))
     line = {"metric": "instance-steps/s", "value": round(value, 2), "unit": "instance-steps/s", "n_gpus": world,
             "steps": r["steps"], "warmup": max(3, args.warmup), "ms_per_step": r["ms_per_step"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x2",
-            "state_dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "describe": r["describe"], "instances_per_gpu": r["instances"],
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+            "dtype": "bf16x2", "state_dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "describe": r["describe"], "instances": r["instances_total"],
+                       "instances_per_gpu": r["instances"],
                        "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
-                       "parallelism": f"replicas x{world}"},
-            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "particle_steps_per_s": round(world * r["particle_steps_per_s"], 1),
+                       "parallelism": f"instances sharded round-robin over {world} GPU(s)"},
+            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "particle_steps_per_s": round(value * r["particle_steps_per_s"] / max(r["value"], 1e-30), 1),
             "gpu_launches": r["gpu_launches"], "kernel_ms": r["kernel_ms"], "roofline": r["roofline"], "e2e": e2e,
             "clocks": clk, "batch": r["batch"]}
     if "accuracy" in r:
@@ -728,8 +769,15 @@ def serve_requests(seconds, rate=200.0, seed=7, n_max=256):
     return out
 
 
-def run_serve(args, local_rank):
-    """Continuous-batching serving run: real-time Poisson arrivals through the engine."""
+def run_serve(args, local_rank, rank=0, world=1):
+    """Continuous-batching serving run: real-time Poisson arrivals through the engine.
+
+    With ``world > 1`` every rank runs its own engine on its round-robin share
+    of the request stream (same arrival times), and rank 0 combines the
+    ranks' completions (replicas.combine_serving): whole-job instance-steps/s
+    over the span from the first submission to the last completion on any
+    rank, latency percentiles over every request.
+    """
     import threading
 
     import torch
@@ -743,7 +791,10 @@ def run_serve(args, local_rank):
     for spec, n in SERVE_DOMAINS:
         dom = make_domain(spec)
         bases.append(cached_basis(dom, n, cache_dir=basis_cache_for(dom.name, n), device="cuda"))
-    reqs = serve_requests(args.serve_seconds, n_max=min(b.n_modes for b in bases))
+    all_reqs = serve_requests(args.serve_seconds, n_max=min(b.n_modes for b in bases))
+    for i, q in enumerate(all_reqs):
+        q["index"] = i
+    reqs = replicas.shard(all_reqs, rank, world) if world > 1 else all_reqs
     # Particle sources: one seeded cloud per domain, each request takes a slice.
     clouds = [initial_particles(b, 2_000_000, 70 + i) for i, b in enumerate(bases)]
     for q in reqs:
@@ -796,7 +847,22 @@ def run_serve(args, local_rank):
     total_steps = sum(q["steps"] for q in reqs)
     first = min(info["t_submit"] for _, info, _ in done)
     last = max(info["t_done"] for _, info, _ in done)
-    out = {"requests": len(reqs), "completed": len(done), "arrival_window_s": args.serve_seconds,
+    if world > 1:
+        # Host-side gather of every rank's completions (CLOCK_MONOTONIC is shared by the processes).
+        mine = {"requests": [reqs[i]["index"] for i, _, _ in done if i is not None], "latencies": lat.tolist(),
+                "steps": total_steps, "first": first, "last": last, "particle_steps": st["particle_steps"]}
+        recs = replicas.gather_objects(mine)
+        job = replicas.combine_serving(recs)
+        lat = np.array([x for r in recs for x in r["latencies"]])
+        total_steps = job["instance_steps"]
+        first = min(r["first"] for r in recs)
+        last = max(r["last"] for r in recs)
+        st["particle_steps"] = sum(r["particle_steps"] for r in recs)
+        st["per_rank_completed"] = job["per_rank_completed"]
+        if rank != 0:
+            return None
+    out = {"requests": len(all_reqs), "completed": int(lat.size), "arrival_window_s": args.serve_seconds,
+           "gpus": world,
            "instance_steps": total_steps, "instance_steps_per_s": round(total_steps / (last - first), 1),
            "particle_steps_per_s": round(st["particle_steps"] / (last - first), 1),
            "p50_latency_s": round(float(np.percentile(lat, 50)), 4),
@@ -1039,20 +1105,19 @@ def main():
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                               device_id=torch.device("cuda", local_rank))
-    if args.workload == SERVE_WORKLOAD:
-        if rank == 0:
-            clocks = ClockSampler(local_rank).start()
-            r = run_serve(args, local_rank)
-            clk = clocks.stop()
-            line = {"metric": "instance-steps/s", "value": r["instance_steps_per_s"], "unit": "instance-steps/s",
-                    "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                    "dtype": "bf16x2", "state_dtype": "f64", "data": "synthetic",
-                    "p50_ms": round(1e3 * r["p50_latency_s"], 2), "p99_ms": round(1e3 * r["p99_latency_s"], 2),
-                    "config": {"workload": SERVE_WORKLOAD, **r.pop("config")}, "serve": r, "clocks": clk}
-            print(json.dumps(line), flush=True)
-        return
     try:
-        if args.workload in BATCH_WORKLOADS:
+        if args.workload == SERVE_WORKLOAD:
+            clocks = ClockSampler(local_rank).start()
+            r = run_serve(args, local_rank, rank, world)
+            clk = clocks.stop()
+            line = None
+            if rank == 0:
+                line = {"metric": "instance-steps/s", "value": r["instance_steps_per_s"], "unit": "instance-steps/s",
+                        "n_gpus": world, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+                        "vs_baseline": None, "dtype": "bf16x2", "state_dtype": "f64", "data": "synthetic",
+                        "p50_ms": round(1e3 * r["p50_latency_s"], 2), "p99_ms": round(1e3 * r["p99_latency_s"], 2),
+                        "config": {"workload": SERVE_WORKLOAD, **r.pop("config")}, "serve": r, "clocks": clk}
+        elif args.workload in BATCH_WORKLOADS:
             line = run_batch_line(args, rank, world, local_rank)
         else:
             line = run_ours(args, rank, world, local_rank)

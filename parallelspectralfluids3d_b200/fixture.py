@@ -159,10 +159,30 @@ class Basis:
         return b
 
 
+def _cuda_index(device) -> int | None:
+    """Device ordinal of a "cuda" / "cuda:K" device string, else None."""
+    d = str(device)
+    if not d.startswith("cuda"):
+        return None
+    return int(d.split(":", 1)[1]) if ":" in d else 0
+
+
 def build_basis(dom: Domain, n_modes: int, device: str = "cpu") -> Basis:
-    """Run the per-domain precompute (eigenbasis, curl, gravity, tensor)."""
+    """Run the per-domain precompute (eigenbasis, curl, gravity, tensor).
+
+    On a CUDA device the whole precompute runs on the GPU
+    (:func:`.precompute.build_basis`: Chebyshev-filtered eigen-solve and the
+    wedge tensor kernels); on ``"cpu"`` it is the host restatement of
+    :mod:`.basis` (SciPy shift-invert ARPACK, FP64 GEMMs).
+    """
     from . import basis as B
 
+    idx = _cuda_index(device)
+    if idx is not None:
+        from . import precompute
+
+        b, _ = precompute.build_basis(dom, n_modes, device=idx)
+        return b
     dom.build()
     lam, phi_I = B.eigenbasis(dom, n_modes)
     phi_full = np.zeros((dom.n_faces, n_modes))
@@ -190,6 +210,11 @@ def rebuild_tensor(b: Basis, device: str | None = None) -> np.ndarray:
             device = "cpu"
     dom = b.domain()
     dom.build()
+    idx = _cuda_index(device)
+    if idx is not None:
+        from . import precompute
+
+        return precompute.advection_tensor(dom, b.phi, b.lam, device=idx)
     phi_full = b.phi_full()
     psi = B.curl_basis(dom, phi_full)
     return B.advection_tensor(dom, phi_full, psi, b.lam, device=device)
