@@ -50,12 +50,21 @@ int cuda_fail(cudaError_t e, const char *what)
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// --------------------------------------------- programmatic dependent launch
+// The three step kernels run back to back in one stream.  Each one loads only
+// constant data (C rows, Phi tiles, face maps) before griddepcontrol.wait, and
+// lets its own dependents launch only after that wait: at most two kernels
+// are in flight, and the second never reads what the first is still writing.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // ------------------------------------------------------- 1. contraction
 // Block b handles mode k = b / S and row slice s = b % S of C_k.  Lane l of a
-// warp owns columns [4l + 128c, 4l + 128c + 4) for c < CH, with w_j in
-// registers; warps walk rows a.  Each lane accumulates
-// sum_a w_a * (C[k][a][j..j+3] . w[j..j+3]) in FP64, so no per-row reduction
-// is needed; one block reduction at the end.
+// warp owns columns [4l + 128c, 4l + 128c + 4) for c < CH; warps walk rows a.
+// Each lane accumulates sum_a w_a * (C[k][a][j..j+3] . w[j..j+3]) in FP64, so
+// no per-row reduction is needed; one block reduction at the end.  The first
+// PF rows of every warp are loaded before the grid-dependency wait (C is
+// constant); the rest stream U rows per batch with w staged in shared memory.
 template <int CH>
 __global__ void __launch_bounds__(256) psf_contract_state(const float *__restrict__ C, int N, int Np, int S,
                                                           double *__restrict__ w, double *__restrict__ dwpart,
@@ -64,13 +73,35 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
                                                           unsigned int *__restrict__ ticket,
                                                           unsigned long long *__restrict__ step_ctr)
 {
+    constexpr int PF = CH <= 2 ? 4 : 2;
+    constexpr int U = CH <= 2 ? 4 : 2;
     __shared__ double red[8];
     __shared__ int is_last;
+    __shared__ double wsh[PSF_MAX_MODES];
     __shared__ double wnew[PSF_MAX_MODES];
 
     const int k = blockIdx.x / S;
     const int s = blockIdx.x - k * S;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rows = (N + S - 1) / S;
+    const int a0 = s * rows;
+    const int a1 = min(N, a0 + rows);
+    const float *Ck = C + (size_t)k * N * Np;
+
+    float4 pre[PF][CH];
+#pragma unroll
+    for (int r = 0; r < PF; ++r) {
+        const int a = a0 + warp + 8 * r;
+        const float4 *row = reinterpret_cast<const float4 *>(Ck + (size_t)a * Np);
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+            pre[r][c] = (a < a1 && c * 128 + lane * 4 < Np) ? __ldg(row + c * 32 + lane)
+                                                            : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    grid_dependency_wait();
+    launch_dependents();
+    for (int i = threadIdx.x; i < N; i += 256) wsh[i] = w[i];
+    __syncthreads();
 
     float wj[CH][4];
 #pragma unroll
@@ -78,29 +109,51 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int col = c * 128 + lane * 4 + q;
-            wj[c][q] = col < N ? (float)w[col] : 0.f;
+            wj[c][q] = col < N ? (float)wsh[col] : 0.f;
         }
     }
-    const int rows = (N + S - 1) / S;
-    const int a0 = s * rows;
-    const int a1 = min(N, a0 + rows);
-    const float *Ck = C + (size_t)k * N * Np;
     double acc = 0.0;
-#pragma unroll 4
-    for (int a = a0 + warp; a < a1; a += 8) {
-        const float4 *row = reinterpret_cast<const float4 *>(Ck + (size_t)a * Np);
-        float part = 0.f;
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            if (c * 128 + lane * 4 < Np) {
-                const float4 v = __ldg(row + c * 32 + lane);
-                part = fmaf(v.x, wj[c][0], part);
-                part = fmaf(v.y, wj[c][1], part);
-                part = fmaf(v.z, wj[c][2], part);
-                part = fmaf(v.w, wj[c][3], part);
+    for (int r = 0; r < PF; ++r) {
+        const int a = a0 + warp + 8 * r;
+        if (a < a1) {
+            float part = 0.f;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                part = fmaf(pre[r][c].x, wj[c][0], part);
+                part = fmaf(pre[r][c].y, wj[c][1], part);
+                part = fmaf(pre[r][c].z, wj[c][2], part);
+                part = fmaf(pre[r][c].w, wj[c][3], part);
+            }
+            acc = fma(wsh[a], (double)part, acc);
+        }
+    }
+    for (int ab = a0 + warp + 8 * PF; ab < a1; ab += 8 * U) {
+        float4 v[U][CH];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int a = ab + 8 * u;
+            const float4 *row = reinterpret_cast<const float4 *>(Ck + (size_t)a * Np);
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                v[u][c] = (a < a1 && c * 128 + lane * 4 < Np) ? __ldg(row + c * 32 + lane)
+                                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int a = ab + 8 * u;
+            if (a < a1) {
+                float part = 0.f;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    part = fmaf(v[u][c].x, wj[c][0], part);
+                    part = fmaf(v[u][c].y, wj[c][1], part);
+                    part = fmaf(v[u][c].z, wj[c][2], part);
+                    part = fmaf(v[u][c].w, wj[c][3], part);
+                }
+                acc = fma(wsh[a], (double)part, acc);
             }
         }
-        acc = fma(w[a], (double)part, acc);
     }
     const double tot = block_sum_256(acc, red);
     if (threadIdx.x == 0) {
@@ -117,7 +170,7 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
     // (psfsolver.cpp:37-59).
     double e1 = 0.0, e2 = 0.0;
     for (int i = threadIdx.x; i < N; i += 256) {
-        const double wi = w[i];
+        const double wi = wsh[i];
         double dw = 0.0;
         for (int q = 0; q < S; ++q) dw += __ldcg(dwpart + i * S + q);
         const double w1 = wi + sp.dt * dw;
@@ -183,6 +236,8 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
             }
         }
     }
+    grid_dependency_wait();
+    launch_dependents();
     for (int i = threadIdx.x; i < N; i += 256) wsm[i] = (float)w[i];
     __syncthreads();
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -231,18 +286,24 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
 }
 
 // Persistent grid (a whole number of resident blocks per SM) striding over
-// the particles, which are stored in cell order.
+// the particles, which are stored in cell order.  A thread's first particle
+// is loaded before the grid-dependency wait: the particles were last written
+// by the previous step's tracer, which completed before this step's
+// contraction passed its own wait.
 __global__ void __launch_bounds__(256, 3) psf_trace(float4 *__restrict__ parts, long long P,
                                                  const int32_t *__restrict__ perm,
                                                  const float2 *__restrict__ pairs, GridDev g, TraceParams tp,
                                                  const unsigned long long *__restrict__ step_ctr)
 {
-    const uint64_t step = *step_ctr - 1ull;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
-        float4 p = parts[i];
-        p = advance_particle(p, g, pairs, tp, step, perm, (size_t)i);
-        parts[i] = p;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float4 p = i < P ? parts[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    grid_dependency_wait();
+    launch_dependents();
+    const uint64_t step = *step_ctr - 1ull;
+    for (bool first = true; i < P; i += stride, first = false) {
+        if (!first) p = parts[i];
+        parts[i] = advance_particle(p, g, pairs, tp, step, perm, (size_t)i);
     }
 }
 
@@ -334,12 +395,31 @@ int launch_contract_state(const PlainDev &d, cudaStream_t st)
 }
 
 
+// Launch configuration of a step kernel that may start while the previous
+// kernel in the stream finishes (programmatic stream serialisation).
+struct PdlLaunch {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    PdlLaunch(unsigned grid, unsigned block, cudaStream_t st)
+    {
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+};
+
 int launch_reconstruct(const PlainDev &d, cudaStream_t st)
 {
     const long long blocks = (d.n_active + 127) / 128;
-    psf_reconstruct<<<(unsigned)blocks, 256, 0, st>>>(d.phiT, d.ldp, d.faces, d.n_active, d.N, d.w, d.u,
-                                                      reinterpret_cast<float *>(d.pairs), d.pair_dst);
-    cudaError_t e = cudaGetLastError();
+    PdlLaunch L((unsigned)blocks, 256, st);
+    cudaError_t e = cudaLaunchKernelEx(&L.cfg, psf_reconstruct, (const float *)d.phiT, (long long)d.ldp,
+                                       (const int32_t *)d.faces, (long long)d.n_active, (int)d.N, (const double *)d.w,
+                                       d.u, reinterpret_cast<float *>(d.pairs), (const int32_t *)d.pair_dst);
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_reconstruct launch");
 }
 
@@ -355,8 +435,10 @@ int launch_trace(const PlainDev &d, cudaStream_t st)
 {
     if (d.P == 0) return PSF_OK;
     const long long blocks = std::min<long long>((d.P + 255) / 256, std::max(1, d.trace_blocks));
-    psf_trace<<<(unsigned)blocks, 256, 0, st>>>(d.parts, d.P, d.perm, d.pairs, d.grid, d.tp, d.step_ctr);
-    cudaError_t e = cudaGetLastError();
+    PdlLaunch L((unsigned)blocks, 256, st);
+    cudaError_t e = cudaLaunchKernelEx(&L.cfg, psf_trace, d.parts, (long long)d.P, (const int32_t *)d.perm,
+                                       (const float2 *)d.pairs, d.grid, d.tp,
+                                       (const unsigned long long *)d.step_ctr);
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_trace launch");
 }
 

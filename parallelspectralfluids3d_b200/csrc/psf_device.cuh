@@ -89,7 +89,7 @@ __device__ __forceinline__ unsigned long long cell_key(const GridDev &g, float p
 // face pairs, each second sample of a lerp stored as its difference to the
 // first (mixf(x, y, t) = fma(t, y - x, x) then costs one FMA).
 struct CellCache {
-    unsigned long long key;
+    float lox, loy, loz, hix, hiy, hiz;  // positions surely in the cell (bounds shrunk by CELL_MARGIN)
     float oxO, oyO, ozO;   // xO, yO, zO
     float oxM, oyM, ozM;   // xM + 1/2, yM + 1/2, zM + 1/2
     float2 x00, dx10, x01, dx11;  // x faces at (xO, yM|yP, zM|zP), differences along y
@@ -97,9 +97,29 @@ struct CellCache {
     float2 zMM, dzMP, zPM, dzPP;  // z faces at (xM|xP, yM|yP, zO), differences along y
 };
 
+// Margin, in voxels, by which the cached cell's bounds are shrunk.  The cell
+// is k = floor(2 (shift + p) / h) per axis; the float rounding of that
+// expression moves a boundary by far less than 1e-3 voxel for grids below
+// ~4000 voxels per axis, so a position inside the shrunk bounds lies in the
+// cached cell for certain.  Any other position gathers its cell again (about
+// 1 % of the stages land within the margin of a boundary); gathering the same
+// cell again reproduces the same cache, so results do not depend on it.
+constexpr float CELL_MARGIN = 1e-3f;
+
+__device__ __forceinline__ void cell_bounds(const GridDev &g, int k, int n, int axis, float &lo, float &hi)
+{
+    const float half_h = 0.5f / g.inv_h;
+    const float margin = CELL_MARGIN / g.inv_h;
+    lo = k <= -1 ? -INFINITY : fmaf((float)k, half_h, -g.shift[axis]) + margin;
+    hi = k >= 2 * n ? INFINITY : fmaf((float)(k + 1), half_h, -g.shift[axis]) - margin;
+}
+
 __device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, int kx, int ky,
                                             int kz, CellCache &c)
 {
+    cell_bounds(g, kx, g.nx, 0, c.lox, c.hix);
+    cell_bounds(g, ky, g.ny, 1, c.loy, c.hiy);
+    cell_bounds(g, kz, g.nz, 2, c.loz, c.hiz);
     const int xO = clampi(kx >> 1, 0, g.nx - 1), yO = clampi(ky >> 1, 0, g.ny - 1), zO = clampi(kz >> 1, 0, g.nz - 1);
     const int xr = (kx - 1) >> 1, yr = (ky - 1) >> 1, zr = (kz - 1) >> 1;
     const int xM = clampi(xr, 0, g.nx - 1), xP = clampi(xr + 1, 0, g.nx - 1);
@@ -172,14 +192,15 @@ __device__ __forceinline__ float3 interpolate(const CellCache &c, const float3 &
 }
 
 // Velocity at a position; `c` carries the last gathered cell, and the
-// samples are loaded again only when the position lies in another cell.
+// samples are loaded again only when the position is not surely inside it.
 __device__ __forceinline__ float3 velocity_cached(const GridDev &g, const float2 *__restrict__ pairs, float px,
                                                   float py, float pz, CellCache &c, bool &have)
 {
-    int kx, ky, kz;
-    const unsigned long long key = cell_key(g, px, py, pz, kx, ky, kz);
-    if (!have || key != c.key) {
-        c.key = key;
+    const bool inside = have && px >= c.lox && px < c.hix && py >= c.loy && py < c.hiy && pz >= c.loz &&
+                        pz < c.hiz;
+    if (!inside) {
+        int kx, ky, kz;
+        cell_key(g, px, py, pz, kx, ky, kz);
         gather_cell(g, pairs, kx, ky, kz, c);
         have = true;
     }
