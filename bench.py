@@ -60,7 +60,7 @@ BATCH_WORKLOADS = {
     "channel48_n256_b64_p1m": dict(
         bases=[(("channel", (48, 48, 48), None), 256)], instances=64, n_modes=lambda i, rng: 256,
         particles=1 << 20, dt=0.005, force0=0.0, integrator=4, seed_w=lambda i: 100 + i,
-        seed_p=lambda i: 10100 + i, full_steps=1000, check=[0, 31, 63], check_particles=[],
+        seed_p=lambda i: 10100 + i, full_steps=1000, check=[0, 31, 63], check_particles=[0, 31, 63],
         describe="48^3 channel, N=256 (C, Phi as BF16 hi+lo), 64 trajectories x 1M particles, RK4, dt=0.005"),
     # Batching form: 512 instances, N ~ U{32..256}, domains in rotation, 16384 particles each.
     "mixed512_p16384": dict(

@@ -87,7 +87,9 @@ def test_gpu_tensor_matches_host_builder(name, c1_basis, small_bases):
     dom = b.domain()
     dom.build()
     got = P.advection_tensor(dom, b.phi, b.lam, device=0)
-    assert np.abs(got - b.C).max() <= TENSOR_TOL * np.abs(b.C).max()
+    phi_full = b.phi_full()
+    want = B.advection_tensor(dom, phi_full, B.curl_basis(dom, phi_full), b.lam)  # host builder, FP64 on the CPU
+    assert np.abs(got - want).max() <= TENSOR_TOL * np.abs(want).max()
 
 
 def test_gpu_tensor_batches_and_splits():
