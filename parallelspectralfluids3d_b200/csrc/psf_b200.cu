@@ -290,7 +290,9 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
 // is loaded before the grid-dependency wait: the particles were last written
 // by the previous step's tracer, which completed before this step's
 // contraction passed its own wait.
-__global__ void __launch_bounds__(256, 3) psf_trace(float4 *__restrict__ parts, long long P,
+constexpr int TRACE_THREADS = 128;
+
+__global__ void __launch_bounds__(TRACE_THREADS, 5) psf_trace(float4 *__restrict__ parts, long long P,
                                                  const int32_t *__restrict__ perm,
                                                  const float2 *__restrict__ pairs, GridDev g, TraceParams tp,
                                                  const unsigned long long *__restrict__ step_ctr)
@@ -426,7 +428,8 @@ int launch_reconstruct(const PlainDev &d, cudaStream_t st)
 int trace_blocks_per_sm()
 {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_trace, 256, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, psf_trace, TRACE_THREADS, 0) != cudaSuccess ||
+        per_sm < 1)
         per_sm = 4;
     return per_sm;
 }
@@ -434,8 +437,9 @@ int trace_blocks_per_sm()
 int launch_trace(const PlainDev &d, cudaStream_t st)
 {
     if (d.P == 0) return PSF_OK;
-    const long long blocks = std::min<long long>((d.P + 255) / 256, std::max(1, d.trace_blocks));
-    PdlLaunch L((unsigned)blocks, 256, st);
+    const long long blocks =
+        std::min<long long>((d.P + TRACE_THREADS - 1) / TRACE_THREADS, std::max(1, d.trace_blocks));
+    PdlLaunch L((unsigned)blocks, TRACE_THREADS, st);
     cudaError_t e = cudaLaunchKernelEx(&L.cfg, psf_trace, d.parts, (long long)d.P, (const int32_t *)d.perm,
                                        (const float2 *)d.pairs, d.grid, d.tp,
                                        (const unsigned long long *)d.step_ctr);

@@ -97,21 +97,18 @@ struct CellCache {
     float2 zMM, dzMP, zPM, dzPP;  // z faces at (xM|xP, yM|yP, zO), differences along y
 };
 
-// Margin, in voxels, by which the cached cell's bounds are shrunk.  The cell
-// is k = floor(2 (shift + p) / h) per axis; the float rounding of that
-// expression moves a boundary by far less than 1e-3 voxel for grids below
-// ~4000 voxels per axis, so a position inside the shrunk bounds lies in the
-// cached cell for certain.  Any other position gathers its cell again (about
-// 1 % of the stages land within the margin of a boundary); gathering the same
-// cell again reproduces the same cache, so results do not depend on it.
-constexpr float CELL_MARGIN = 1e-3f;
-
+// Bounds of a cached cell, shrunk by CELL_MARGIN voxels (GridDev::margin).
+// The cell is k = floor(2 (shift + p) / h) per axis; the float rounding of
+// that expression moves a boundary by far less than 1e-3 voxel for grids
+// below ~4000 voxels per axis, so a position inside the shrunk bounds lies in
+// the cached cell for certain.  Any other position gathers its cell again
+// (about 1 % of the stages land within the margin of a boundary); gathering
+// the same cell again reproduces the same cache, so results do not depend on
+// it.
 __device__ __forceinline__ void cell_bounds(const GridDev &g, int k, int n, int axis, float &lo, float &hi)
 {
-    const float half_h = 0.5f / g.inv_h;
-    const float margin = CELL_MARGIN / g.inv_h;
-    lo = k <= -1 ? -INFINITY : fmaf((float)k, half_h, -g.shift[axis]) + margin;
-    hi = k >= 2 * n ? INFINITY : fmaf((float)(k + 1), half_h, -g.shift[axis]) - margin;
+    lo = k <= -1 ? -INFINITY : fmaf((float)k, g.half_h, -g.shift[axis]) + g.margin;
+    hi = k >= 2 * n ? INFINITY : fmaf((float)(k + 1), g.half_h, -g.shift[axis]) - g.margin;
 }
 
 __device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, int kx, int ky,
@@ -135,18 +132,24 @@ __device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__re
     const float2 *__restrict__ pxp = pairs;
     const float2 *__restrict__ pyp = pairs + V;
     const float2 *__restrict__ pzp = pairs + 2 * (size_t)V;
-    const float2 x00 = __ldg(pxp + voxel(g, xO, yM, zM));
-    const float2 x10 = __ldg(pxp + voxel(g, xO, yP, zM));
-    const float2 x01 = __ldg(pxp + voxel(g, xO, yM, zP));
-    const float2 x11 = __ldg(pxp + voxel(g, xO, yP, zP));
-    const float2 yM0 = __ldg(pyp + voxel(g, xM, yO, zM));
-    const float2 yP0 = __ldg(pyp + voxel(g, xP, yO, zM));
-    const float2 yM1 = __ldg(pyp + voxel(g, xM, yO, zP));
-    const float2 yP1 = __ldg(pyp + voxel(g, xP, yO, zP));
-    const float2 zMM = __ldg(pzp + voxel(g, xM, yM, zO));
-    const float2 zMP = __ldg(pzp + voxel(g, xM, yP, zO));
-    const float2 zPM = __ldg(pzp + voxel(g, xP, yM, zO));
-    const float2 zPP = __ldg(pzp + voxel(g, xP, yP, zO));
+    // Each component's four voxels differ from its base voxel by the steps
+    // M -> P along two axes (0 where the clamp merges them).
+    const uint32_t bx = voxel(g, xO, yM, zM), by = voxel(g, xM, yO, zM), bz = voxel(g, xM, yM, zO);
+    const uint32_t dx = (uint32_t)(xP - xM);
+    const uint32_t dy = (uint32_t)(yP - yM) * (uint32_t)g.nx;
+    const uint32_t dz = (uint32_t)(zP - zM) * ((uint32_t)g.nx * (uint32_t)g.ny);
+    const float2 x00 = __ldg(pxp + bx);
+    const float2 x10 = __ldg(pxp + bx + dy);
+    const float2 x01 = __ldg(pxp + bx + dz);
+    const float2 x11 = __ldg(pxp + bx + dy + dz);
+    const float2 yM0 = __ldg(pyp + by);
+    const float2 yP0 = __ldg(pyp + by + dx);
+    const float2 yM1 = __ldg(pyp + by + dz);
+    const float2 yP1 = __ldg(pyp + by + dx + dz);
+    const float2 zMM = __ldg(pzp + bz);
+    const float2 zMP = __ldg(pzp + bz + dy);
+    const float2 zPM = __ldg(pzp + bz + dx);
+    const float2 zPP = __ldg(pzp + bz + dx + dy);
     c.x00 = x00;
     c.dx10 = make_float2(x10.x - x00.x, x10.y - x00.y);
     c.x01 = x01;
