@@ -106,7 +106,7 @@ class OracleRollout:
     """FP64 reference-semantics rollout of one instance on a basis."""
 
     def __init__(self, b, w0, particles=None, dt=0.01, viscosity=0.0, flags=FLAG_RENORM,
-                 integrator=1, lifetime=np.inf, seed=0, forcing=None, reconstruct=True):
+                 integrator=1, lifetime=np.inf, seed=0, forcing=None, reconstruct=True, positions="f64"):
         self.b = b
         self.N = b.n_modes
         self.C = np.ascontiguousarray(b.C, dtype=np.float64)
@@ -129,6 +129,12 @@ class OracleRollout:
         self.grid = grid_of(b)
         self.step_index = 0
         self.reconstruct = bool(reconstruct)
+        # "f64": positions carried in FP64 (the ground truth).  "f32": rounded to
+        # FP32 after every step, as the reference stores them (glm::vec4,
+        # Graphics/Particle/Particle.h:14; psfsolver.cpp:215).
+        if positions not in ("f64", "f32"):
+            raise ValueError("positions must be 'f64' or 'f32'")
+        self.positions = positions
         if particles is None:
             particles = np.zeros((0, 4), dtype=np.float32)
         particles = np.asarray(particles, dtype=np.float32)
@@ -157,6 +163,8 @@ class OracleRollout:
         for _ in range(n):
             self.coeff_step()
             self.trace()
+            if self.positions == "f32":
+                self.pos[...] = self.pos.astype(np.float32)
             self.step_index += 1
         return self
 

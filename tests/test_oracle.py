@@ -159,3 +159,20 @@ def test_respawn_formula():
         assert r.pos[i, 1] == np.float32(np.float32(-0.5) + np.float32(0.2))
         assert r.pos[i, 2] == np.float32((h(i, 3) / 1024.0 - 0.5) * 0.25)
         assert r.life[i] == np.float32(60.0 * (h(i, 2) / 1024.0))
+
+
+def test_fp32_position_mode_stores_float_positions(small_bases):
+    """positions="f32" rounds the state to FP32 after every step, as the reference's
+    glm::vec4 particle buffer does; with FP64 positions the state is not float-exact."""
+    from parallelspectralfluids3d_b200.fixture import initial_coefficients, initial_particles
+
+    b = small_bases["sphere10"]
+    w0 = initial_coefficients(b.n_modes, 0)
+    parts = initial_particles(b, 300, 1)
+    r32 = O.OracleRollout(b, w0, parts, dt=0.05, integrator=4, positions="f32").step(5)
+    r64 = O.OracleRollout(b, w0, parts, dt=0.05, integrator=4).step(5)
+    assert np.array_equal(r32.pos, r32.pos.astype(np.float32).astype(np.float64))
+    assert not np.array_equal(r64.pos, r64.pos.astype(np.float32).astype(np.float64))
+    assert np.abs(r32.pos - r64.pos).max() < 1e-5
+    with pytest.raises(ValueError):
+        O.OracleRollout(b, w0, parts, positions="f16")
