@@ -139,12 +139,24 @@ psf::GridDev make_grid_dev(const psf_grid &g)
 using psf::fold_signs;
 using psf::n_faces_of;
 
+// A context keeps two coefficient buffers.  `vis` holds the state the caller
+// sees (w^n after n steps); the other holds w^{n+1}, already computed (the
+// contraction "primes" it whenever the state, the forcing or the parameters
+// change).  A step reconstructs and traces with w^{n+1} and, on a parallel
+// branch of the same graph, contracts w^{n+1} into w^{n+2} in the buffer it
+// leaves behind; then the buffers swap roles.  Each buffer carries its step
+// count, so the tracer reads the count of the buffer no kernel writes.
 struct psf_ctx {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaStream_t side = nullptr;   // the contraction's branch during graph capture
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaGraph_t graphs[2] = {nullptr, nullptr};
+    cudaGraphExec_t execs[2] = {nullptr, nullptr};  // index: the buffer the step reconstructs from
+    double *wbuf[2] = {nullptr, nullptr};
+    unsigned long long *ctrbuf = nullptr;           // [2] completed steps of each buffer's state
+    int vis = 0;
     bool have_state = false;
     psf_grid grid{};
     psf_params params{};
@@ -158,14 +170,29 @@ struct psf_ctx {
     {
         drop_graph();
         for (void *p : allocs) cudaFree(p);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
     void drop_graph()
     {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
+        for (int p = 0; p < 2; ++p) {
+            if (execs[p]) cudaGraphExecDestroy(execs[p]);
+            if (graphs[p]) cudaGraphDestroy(graphs[p]);
+            execs[p] = nullptr;
+            graphs[p] = nullptr;
+        }
+    }
+    // Device view of a step that reconstructs from buffer p and contracts it into the other one.
+    psf::PlainDev dev_for(int p) const
+    {
+        psf::PlainDev v = d;
+        v.w = wbuf[p];
+        v.w_next = wbuf[1 - p];
+        v.step_ctr = ctrbuf + p;
+        v.step_ctr_next = ctrbuf + (1 - p);
+        return v;
     }
     template <class T>
     int alloc(T **p, size_t count)
@@ -198,6 +225,12 @@ struct psf_ctx {
         if (e_ != cudaSuccess) return psf::cuda_fail(e_, #x); \
     } while (0)
 
+// w^{n+1} from the visible w^n into the other buffer (stream-ordered).
+static int prime(psf_ctx *c)
+{
+    return psf::launch_contract_state(c->dev_for(c->vis), c->stream);
+}
+
 static int apply_params(psf_ctx *c, const psf_params &p)
 {
     if (!(p.timestep > 0.0) || !std::isfinite(p.timestep))
@@ -215,6 +248,11 @@ static int apply_params(psf_ctx *c, const psf_params &p)
     c->d.tp.rk4 = p.integrator == PSF_RK4;
     c->d.tp.seed = p.seed;
     c->drop_graph();
+    if (c->have_state) {
+        PSF_CHECK(prime(c));
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return psf::cuda_fail(e, "priming the next state");
+    }
     return PSF_OK;
 }
 
@@ -225,22 +263,34 @@ static int sync_stream(psf_ctx *c)
     return PSF_OK;
 }
 
-static int build_graph(psf_ctx *c)
+// One step as a graph: reconstruction -> tracer on the context's stream,
+// and beside them the next step's contraction on a forked branch.
+static int build_graph(psf_ctx *c, int p)
 {
-    if (c->exec) return PSF_OK;
+    if (c->execs[p]) return PSF_OK;
+    const psf::PlainDev dp = c->dev_for(p);
     PSF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = psf::launch_contract_state(c->d, c->stream);
-    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->d, c->stream);
-    if (rc == PSF_OK) rc = psf::launch_trace(c->d, c->stream);
+    int rc = PSF_OK;
+    cudaError_t e = cudaEventRecord(c->fork, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->fork, 0);
+    if (e != cudaSuccess) rc = psf::cuda_fail(e, "forking the contraction branch");
+    if (rc == PSF_OK) rc = psf::launch_contract_state(dp, c->side);
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(dp, c->stream, /*after_kernel=*/false);
+    if (rc == PSF_OK) rc = psf::launch_trace(dp, c->stream);
+    if (rc == PSF_OK) {
+        e = cudaEventRecord(c->join, c->side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->join, 0);
+        if (e != cudaSuccess) rc = psf::cuda_fail(e, "joining the contraction branch");
+    }
     cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    e = cudaStreamEndCapture(c->stream, &g);
     if (rc != PSF_OK) {
         if (g) cudaGraphDestroy(g);
         return rc;
     }
     if (e != cudaSuccess) return psf::cuda_fail(e, "cudaStreamEndCapture");
-    c->graph = g;
-    PSF_CUDA(cudaGraphInstantiate(&c->exec, c->graph, 0));
+    c->graphs[p] = g;
+    PSF_CUDA(cudaGraphInstantiate(&c->execs[p], g, 0));
     return PSF_OK;
 }
 
@@ -315,6 +365,9 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaSetDevice"));
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
     if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaStreamCreate"));
     c->grid = g;
     if ((rc = fold_signs(g, b->sign_bits, c->sigma)) != PSF_OK) return bail(rc);
@@ -347,11 +400,12 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         int32_t *faces = nullptr;
         double *lam = nullptr, *force = nullptr;
         if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phiT, hP.size())) ||
-            (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&d.w, (size_t)N)) ||
+            (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&c->wbuf[0], 2 * (size_t)N)) ||
             (rc = c->alloc(&d.dwpart, (size_t)N * d.S)) || (rc = c->alloc(&lam, (size_t)N)) ||
             (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
-            (rc = c->alloc(&d.step_ctr, 1)) || (rc = c->alloc(&d.u, (size_t)F)))
+            (rc = c->alloc(&c->ctrbuf, 2)) || (rc = c->alloc(&d.u, (size_t)F)))
             return bail(rc);
+        c->wbuf[1] = c->wbuf[0] + N;
         // Per-voxel face pairs read by the tracer, and where each active face goes.
         std::vector<int32_t> hdst;
         psf::face_pair_slots(g, b->active_faces, b->n_active, hdst);
@@ -372,8 +426,9 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
             (e = cudaMemcpyAsync(phiT, hP.data(), hP.size() * 4, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(faces, b->active_faces, (size_t)b->n_active * 4, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(lam, b->eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st)) ||
-            (e = cudaMemsetAsync(force, 0, (size_t)N * 8, st)) || (e = cudaMemsetAsync(d.w, 0, (size_t)N * 8, st)) ||
-            (e = cudaMemsetAsync(d.ticket, 0, 4, st)) || (e = cudaMemsetAsync(d.step_ctr, 0, 8, st)) ||
+            (e = cudaMemsetAsync(force, 0, (size_t)N * 8, st)) ||
+            (e = cudaMemsetAsync(c->wbuf[0], 0, 2 * (size_t)N * 8, st)) ||
+            (e = cudaMemsetAsync(d.ticket, 0, 4, st)) || (e = cudaMemsetAsync(c->ctrbuf, 0, 16, st)) ||
             (e = cudaMemsetAsync(d.u, 0, (size_t)F * 4, st)) || (e = cudaStreamSynchronize(st)))
             return bail(psf::cuda_fail(e, "basis upload"));
     } catch (const std::bad_alloc &) {
@@ -409,7 +464,8 @@ int psf_set_state(psf_ctx *c, const double *w, int32_t n)
     if (!c || !w) return fail(PSF_ERR_INVALID, "null argument");
     if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CUDA(cudaMemcpyAsync(c->d.w, w, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    PSF_CUDA(cudaMemcpyAsync(c->wbuf[c->vis], w, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    PSF_CHECK(prime(c));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
     c->have_state = true;
     return PSF_OK;
@@ -420,7 +476,7 @@ int psf_get_state(psf_ctx *c, double *w, int32_t n)
     if (!c || !w) return fail(PSF_ERR_INVALID, "null argument");
     if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CUDA(cudaMemcpyAsync(w, c->d.w, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    PSF_CUDA(cudaMemcpyAsync(w, c->wbuf[c->vis], (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
     PSF_CHECK(sync_stream(c));
     return PSF_OK;
 }
@@ -432,6 +488,7 @@ int psf_set_forcing(psf_ctx *c, const double *f, int32_t n)
     PSF_CUDA(cudaSetDevice(c->device));
     PSF_CUDA(cudaMemcpyAsync(const_cast<double *>(c->d.force), f, (size_t)n * 8, cudaMemcpyHostToDevice,
                              c->stream));
+    if (c->have_state) PSF_CHECK(prime(c));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
     return PSF_OK;
 }
@@ -507,8 +564,13 @@ int psf_step(psf_ctx *c, int32_t nsteps)
     if (nsteps < 0) return fail(PSF_ERR_INVALID, "nsteps must be >= 0");
     if (!c->have_state) return fail(PSF_ERR_STATE, "psf_set_state must be called before stepping");
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CHECK(build_graph(c));
-    for (int32_t i = 0; i < nsteps; ++i) PSF_CUDA(cudaGraphLaunch(c->exec, c->stream));
+    PSF_CHECK(build_graph(c, 0));
+    PSF_CHECK(build_graph(c, 1));
+    for (int32_t i = 0; i < nsteps; ++i) {
+        const int p = 1 - c->vis;  // the buffer holding w^{n+1}
+        PSF_CUDA(cudaGraphLaunch(c->execs[p], c->stream));
+        c->vis = p;
+    }
     return PSF_OK;
 }
 
@@ -544,15 +606,20 @@ int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
     for (int i = 0; i <= nk; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
     int rc = PSF_OK;
     cudaStream_t st = c->stream;
+    // The kernels of one step, one after the other: the contraction of the
+    // next state, then the reconstruction and the tracer of this one.
+    const int p = 1 - c->vis;
+    const psf::PlainDev dp = c->dev_for(p);
     cudaEventRecord(ev[0], st);
-    if (rc == PSF_OK) rc = psf::launch_contract_state(c->d, st);
+    if (rc == PSF_OK) rc = psf::launch_contract_state(dp, st);
     cudaEventRecord(ev[1], st);
-    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->d, st);
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(dp, st, /*after_kernel=*/false);
     cudaEventRecord(ev[2], st);
     if (rc == PSF_OK && nk == 3) {
-        rc = psf::launch_trace(c->d, st);
+        rc = psf::launch_trace(dp, st);
         cudaEventRecord(ev[3], st);
     }
+    if (rc == PSF_OK) c->vis = p;
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");
     for (int i = 0; rc == PSF_OK && i < nk; ++i) {

@@ -67,11 +67,13 @@ __device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontr
 // constant); the rest stream U rows per batch with w staged in shared memory.
 template <int CH>
 __global__ void __launch_bounds__(256) psf_contract_state(const float *__restrict__ C, int N, int Np, int S,
-                                                          double *__restrict__ w, double *__restrict__ dwpart,
+                                                          const double *w, double *w_next,
+                                                          double *__restrict__ dwpart,
                                                           const double *__restrict__ lam,
                                                           const double *__restrict__ force, StateParams sp,
                                                           unsigned int *__restrict__ ticket,
-                                                          unsigned long long *__restrict__ step_ctr)
+                                                          const unsigned long long *step_ctr,
+                                                          unsigned long long *step_ctr_next)
 {
     constexpr int PF = CH <= 2 ? 4 : 2;
     constexpr int U = CH <= 2 ? 4 : 2;
@@ -185,11 +187,12 @@ __global__ void __launch_bounds__(256) psf_contract_state(const float *__restric
         double v = wnew[i] * scale;
         v *= exp(sp.visc_signed * lam[i] * sp.dt);
         if (sp.flags & PSF_FLAG_FORCING) v += sp.dt * force[i];
-        w[i] = v;
+        w_next[i] = v;
     }
     if (threadIdx.x == 0) {
         *ticket = 0u;
-        *step_ctr += 1ull;
+        const unsigned long long n = *step_ctr;
+        *step_ctr_next = n + 1ull;
     }
 }
 
@@ -376,8 +379,9 @@ int launch_contract_state(const PlainDev &d, cudaStream_t st)
     const dim3 grid(d.N * d.S), block(256);
 #define PSF_CASE(n)                                                                                   \
     case n:                                                                                           \
-        psf_contract_state<n><<<grid, block, 0, st>>>(d.C, d.N, d.Np, d.S, d.w, d.dwpart, d.lam,     \
-                                                      d.force, d.sp, d.ticket, d.step_ctr);          \
+        psf_contract_state<n><<<grid, block, 0, st>>>(d.C, d.N, d.Np, d.S, d.w, d.w_next, d.dwpart,  \
+                                                      d.lam, d.force, d.sp, d.ticket, d.step_ctr,    \
+                                                      d.step_ctr_next);                              \
         break;
     switch (CH) {
         PSF_CASE(1)
@@ -415,10 +419,11 @@ struct PdlLaunch {
     }
 };
 
-int launch_reconstruct(const PlainDev &d, cudaStream_t st)
+int launch_reconstruct(const PlainDev &d, cudaStream_t st, bool after_kernel)
 {
     const long long blocks = (d.n_active + 127) / 128;
     PdlLaunch L((unsigned)blocks, 256, st);
+    if (!after_kernel) L.cfg.numAttrs = 0;
     cudaError_t e = cudaLaunchKernelEx(&L.cfg, psf_reconstruct, (const float *)d.phiT, (long long)d.ldp,
                                        (const int32_t *)d.faces, (long long)d.n_active, (int)d.N, (const double *)d.w,
                                        d.u, reinterpret_cast<float *>(d.pairs), (const int32_t *)d.pair_dst);

@@ -104,11 +104,15 @@ struct CellCache {
 // the cached cell for certain.  Any other position gathers its cell again
 // (about 1 % of the stages land within the margin of a boundary); gathering
 // the same cell again reproduces the same cache, so results do not depend on
-// it.
+// it.  After the clamp to the grid, cells k = -1 and 0 have the same stencil
+// (every index clamps to 0), and so do k = 2n - 1 and 2n (every index clamps
+// to n - 1): each pair is one cell here, open towards the outside.  Particles
+// clamped onto a wall sit exactly on such a boundary, and stay there (the
+// normal face velocity is zero on the wall), so they must not regather.
 __device__ __forceinline__ void cell_bounds(const GridDev &g, int k, int n, int axis, float &lo, float &hi)
 {
-    lo = k <= -1 ? -INFINITY : fmaf((float)k, g.half_h, -g.shift[axis]) + g.margin;
-    hi = k >= 2 * n ? INFINITY : fmaf((float)(k + 1), g.half_h, -g.shift[axis]) - g.margin;
+    lo = k <= 0 ? -INFINITY : fmaf((float)k, g.half_h, -g.shift[axis]) + g.margin;
+    hi = k >= 2 * n - 1 ? INFINITY : fmaf((float)(k + 1), g.half_h, -g.shift[axis]) - g.margin;
 }
 
 __device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, int kx, int ky,

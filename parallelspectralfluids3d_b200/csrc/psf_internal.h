@@ -52,10 +52,15 @@ struct PlainDev {
     const float *C;      // [N][N][Np]
     const float *phiT;   // [ldp / 64][N][64]: 64-face tiles, each mode-major; signed
     const int32_t *faces;
-    double *w, *dwpart;
+    // The contraction reads w (and its step count) and writes the updated
+    // state to w_next (and the count + 1); the reconstruction reads w.  A
+    // context keeps two state buffers and alternates them, so the next
+    // step's contraction runs beside this step's reconstruction and tracer;
+    // w_next == w updates in place.
+    double *w, *w_next, *dwpart;
     const double *lam, *force;
     unsigned int *ticket;
-    unsigned long long *step_ctr;
+    unsigned long long *step_ctr, *step_ctr_next;
     float *u;            // [n_faces], signed
     float2 *pairs;       // [3][V] per-voxel face pairs (x, y, z), signed
     const int32_t *pair_dst;  // [n_active][2] float indices into pairs of each active face
@@ -104,7 +109,9 @@ int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 
 int launch_contract_state(const PlainDev &d, cudaStream_t st);
-int launch_reconstruct(const PlainDev &d, cudaStream_t st);
+// `after_kernel`: the launch directly follows a kernel in the stream and may
+// start during that kernel's tail (programmatic dependent launch).
+int launch_reconstruct(const PlainDev &d, cudaStream_t st, bool after_kernel = true);
 int launch_trace(const PlainDev &d, cudaStream_t st);
 int trace_blocks_per_sm();
 int sort_particles_temp_bytes(long long P, size_t *bytes);

@@ -146,11 +146,13 @@ extern "C" int psf_coeff_step_static(const float *advection_f32, int32_t n_modes
     d.S = S;
     d.C = advection_f32;
     d.w = w;
+    d.w_next = w;  // in place
     d.lam = eigenvalues;
     d.force = forcing;
     d.dwpart = reinterpret_cast<double *>(scratch);
     d.ticket = reinterpret_cast<unsigned int *>(scratch + kTicketOffset);
     d.step_ctr = reinterpret_cast<unsigned long long *>(scratch + kCounterOffset);
+    d.step_ctr_next = d.step_ctr;
     d.sp.dt = params->timestep;
     d.sp.visc_signed = (params->flags & PSF_FLAG_DECAY_NEG) ? -params->viscosity : params->viscosity;
     d.sp.flags = params->flags;

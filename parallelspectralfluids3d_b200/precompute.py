@@ -281,8 +281,13 @@ def wedge_data(dom: Domain):
 
 
 def advection_tensor(dom: Domain, phi_I: np.ndarray, lam: np.ndarray, device=0, budget_bytes: int = 8 << 30,
-                     return_device: bool = False):
-    """``C[k][a][j]`` (FP64, ``(N, N, N)``) on the GPU from the interior-face basis ``phi_I``."""
+                     return_device: bool = False, stats: dict | None = None):
+    """``C[k][a][j]`` (FP64, ``(N, N, N)``) on the GPU from the interior-face basis ``phi_I``.
+
+    ``stats``, when given, receives the device time of the tensor kernels
+    (``kernel_ms``), the edges with wedge terms, the mode batch and the GEMM's
+    FP64 operation count (``gemm_flops`` = 2 N^2 ldn E over all batches).
+    """
     import torch
 
     dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
@@ -309,9 +314,16 @@ def advection_tensor(dom: Domain, phi_I: np.ndarray, lam: np.ndarray, device=0, 
     L.check(lib.psf_pre_advection_workspace(ct.byref(desc), kb, ct.byref(ws_bytes)))
     ws = torch.empty((ws_bytes.value + 255) // 8, dtype=torch.float64, device=dev)
     C = torch.empty((N, N, N), dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
     L.check(lib.psf_pre_advection_tensor(ct.byref(desc), kb, ws.data_ptr(), ws_bytes.value, C.data_ptr(),
                                          _stream_ptr(dev)))
+    e1.record(st)
     torch.cuda.synchronize(dev)
+    if stats is not None:
+        stats.update(kernel_ms=e0.elapsed_time(e1), edges=E, k_batch=kb, ldn=ldn,
+                     gemm_flops=2.0 * N * (N * ldn) * ((E + 15) // 16 * 16))
     del ws
     return C if return_device else C.cpu().numpy()
 
@@ -328,9 +340,11 @@ def build_basis(dom: Domain, n_modes: int, device=0, **kw):
     phi_full = np.zeros((dom.n_faces, n_modes))
     phi_full[dom.interior_faces] = phi_I
     grav = B.gravity_coefficients(dom, phi_full)
-    C = advection_tensor(dom, phi_I, lam, device=device)
+    tstats = {}
+    C = advection_tensor(dom, phi_I, lam, device=device, stats=tstats)
     t3 = time.perf_counter()
-    stats.update(domain_s=t1 - t0, eigensolve_s=t2 - t1, tensor_s=t3 - t2)
+    stats.update(domain_s=t1 - t0, eigensolve_s=t2 - t1, tensor_s=t3 - t2,
+                 **{f"tensor_{k}": v for k, v in tstats.items()})
     b = Basis(dom.dims, dom.h, dom.aabb_min, dom.aabb_max, dom.interior_faces.astype(np.int32), lam, grav, phi_I,
               C, dom.sign_bits, dom.inside.ravel().astype(np.uint8), name=dom.name)
     return b, stats

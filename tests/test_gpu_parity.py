@@ -118,3 +118,54 @@ def test_errors_are_status_codes(c1_basis):
     with pytest.raises(L.PSFError):
         ctx.set_params(bad)
     ctx.close()
+
+
+def test_profiled_steps_equal_graph_steps(small_bases):
+    """psf_profile_step runs a step kernel by kernel; mixed with graph steps it gives the same states."""
+    b = small_bases["sphere12x10x9"]
+    w0 = initial_coefficients(b.n_modes, 4)
+    parts = initial_particles(b, 400, 4)
+    outs = []
+    for plan in (["g"] * 6, ["p", "g", "p", "p", "g", "p"]):
+        ctx = Context(b, L.make_params(dt=0.03))
+        ctx.set_state(w0)
+        ctx.set_particles(parts)
+        for k in plan:
+            ctx.step(1) if k == "g" else ctx.profile_step()
+        outs.append((ctx.get_state(), ctx.get_particles(), ctx.get_velocity()))
+        ctx.close()
+    for a, c in zip(outs[0], outs[1]):
+        assert np.array_equal(a, c)
+
+
+def test_changes_between_steps_take_effect_at_the_next_step(small_bases):
+    """Each step's state update is prepared one step ahead; changing the time step,
+    the forcing or the state between steps must still act from the next step on."""
+    b = small_bases["sphere12x10x9"]
+    w0 = initial_coefficients(b.n_modes, 6)
+    w1 = initial_coefficients(b.n_modes, 7)
+    f = np.zeros(b.n_modes)
+    f[1] = 0.5
+    ctx = Context(b, L.make_params(dt=0.02))
+    ctx.set_state(w0)
+    ctx.step(3)
+    ctx.set_params(L.make_params(dt=0.05))
+    ctx.step(2)
+    ctx.set_forcing(f)
+    ctx.set_params(L.make_params(dt=0.05, flags=L.PSF_FLAG_RENORM | L.PSF_FLAG_FORCING))
+    ctx.step(2)
+    got_a = ctx.get_state()
+    ctx.set_state(w1)
+    assert np.array_equal(ctx.get_state(), w1)
+    ctx.step(4)
+    got_b = ctx.get_state()
+    ctx.close()
+    ref = O.OracleRollout(b, w0, None, dt=0.02, reconstruct=False).step(3)
+    ref.dt = 0.05
+    ref.step(2)
+    ref.force = np.ascontiguousarray(f)
+    ref.flags |= O.FLAG_FORCING
+    ref.step(2)
+    assert rel_err(got_a, ref.w) <= W_TOL
+    ref_b = O.OracleRollout(b, w1, None, dt=0.05, forcing=f, reconstruct=False).step(4)
+    assert rel_err(got_b, ref_b.w) <= W_TOL
