@@ -129,8 +129,6 @@ psf::GridDev make_grid_dev(const psf_grid &g)
     }
     d.yoff = (uint32_t)((nz + 1) * nx * ny);
     d.xoff = (uint32_t)((nz + 1) * nx * ny + (ny + 1) * nx * nz);
-    d.half_h = (float)(0.5 * g.resolution);
-    d.margin = (float)((double)CELL_MARGIN * g.resolution);
     return d;
 }
 

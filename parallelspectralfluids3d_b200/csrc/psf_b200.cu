@@ -293,9 +293,9 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
 // is loaded before the grid-dependency wait: the particles were last written
 // by the previous step's tracer, which completed before this step's
 // contraction passed its own wait.
-constexpr int TRACE_THREADS = 128;
+constexpr int TRACE_THREADS = 256;
 
-__global__ void __launch_bounds__(TRACE_THREADS, 5) psf_trace(float4 *__restrict__ parts, long long P,
+__global__ void __launch_bounds__(TRACE_THREADS, 3) psf_trace(float4 *__restrict__ parts, long long P,
                                                  const int32_t *__restrict__ perm,
                                                  const float2 *__restrict__ pairs, GridDev g, TraceParams tp,
                                                  const unsigned long long *__restrict__ step_ctr)

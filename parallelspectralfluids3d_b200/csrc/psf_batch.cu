@@ -556,11 +556,6 @@ __global__ void __launch_bounds__(128, 5) psf_batch_trace(const GroupDev *__rest
     uint64_t step = 0;
     const float2 *pairs = nullptr;
     const GroupDev *G = nullptr;
-    // The slot's grid constants, copied once per slot change: read through
-    // the group pointer they would be loaded again at every use.
-    GridDev grid;
-    float4 *parts = nullptr;
-    const int32_t *perm = nullptr;
     for (long long gi = (long long)blockIdx.x * blockDim.x + threadIdx.x; gi < total; gi += stride) {
         if (cur < 0 || gi >= pre[cur + 1]) {
             int lo = cur < 0 ? 0 : cur;
@@ -590,13 +585,12 @@ __global__ void __launch_bounds__(128, 5) psf_batch_trace(const GroupDev *__rest
             tp.seed = s.seed;
             step = s.step - 1ull;
             pairs = G->pairs + (size_t)s.slot * 3 * (size_t)G->V;
-            grid = G->grid;
-            parts = G->parts;
-            perm = G->perm;
         }
         if (!live) continue;
         const size_t idx = base + (size_t)gi;
-        parts[idx] = advance_particle(parts[idx], grid, pairs, tp, step, perm, idx);
+        float4 p = G->parts[idx];
+        p = advance_particle(p, G->grid, pairs, tp, step, G->perm, idx);
+        G->parts[idx] = p;
     }
 }
 

@@ -89,7 +89,7 @@ __device__ __forceinline__ unsigned long long cell_key(const GridDev &g, float p
 // face pairs, each second sample of a lerp stored as its difference to the
 // first (mixf(x, y, t) = fma(t, y - x, x) then costs one FMA).
 struct CellCache {
-    float lox, loy, loz, hix, hiy, hiz;  // positions surely in the cell (bounds shrunk by CELL_MARGIN)
+    unsigned long long key;
     float oxO, oyO, ozO;   // xO, yO, zO
     float oxM, oyM, ozM;   // xM + 1/2, yM + 1/2, zM + 1/2
     float2 x00, dx10, x01, dx11;  // x faces at (xO, yM|yP, zM|zP), differences along y
@@ -97,30 +97,9 @@ struct CellCache {
     float2 zMM, dzMP, zPM, dzPP;  // z faces at (xM|xP, yM|yP, zO), differences along y
 };
 
-// Bounds of a cached cell, shrunk by CELL_MARGIN voxels (GridDev::margin).
-// The cell is k = floor(2 (shift + p) / h) per axis; the float rounding of
-// that expression moves a boundary by far less than 1e-3 voxel for grids
-// below ~4000 voxels per axis, so a position inside the shrunk bounds lies in
-// the cached cell for certain.  Any other position gathers its cell again
-// (about 1 % of the stages land within the margin of a boundary); gathering
-// the same cell again reproduces the same cache, so results do not depend on
-// it.  After the clamp to the grid, cells k = -1 and 0 have the same stencil
-// (every index clamps to 0), and so do k = 2n - 1 and 2n (every index clamps
-// to n - 1): each pair is one cell here, open towards the outside.  Particles
-// clamped onto a wall sit exactly on such a boundary, and stay there (the
-// normal face velocity is zero on the wall), so they must not regather.
-__device__ __forceinline__ void cell_bounds(const GridDev &g, int k, int n, int axis, float &lo, float &hi)
-{
-    lo = k <= 0 ? -INFINITY : fmaf((float)k, g.half_h, -g.shift[axis]) + g.margin;
-    hi = k >= 2 * n - 1 ? INFINITY : fmaf((float)(k + 1), g.half_h, -g.shift[axis]) - g.margin;
-}
-
 __device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__restrict__ pairs, int kx, int ky,
                                             int kz, CellCache &c)
 {
-    cell_bounds(g, kx, g.nx, 0, c.lox, c.hix);
-    cell_bounds(g, ky, g.ny, 1, c.loy, c.hiy);
-    cell_bounds(g, kz, g.nz, 2, c.loz, c.hiz);
     const int xO = clampi(kx >> 1, 0, g.nx - 1), yO = clampi(ky >> 1, 0, g.ny - 1), zO = clampi(kz >> 1, 0, g.nz - 1);
     const int xr = (kx - 1) >> 1, yr = (ky - 1) >> 1, zr = (kz - 1) >> 1;
     const int xM = clampi(xr, 0, g.nx - 1), xP = clampi(xr + 1, 0, g.nx - 1);
@@ -136,24 +115,18 @@ __device__ __forceinline__ void gather_cell(const GridDev &g, const float2 *__re
     const float2 *__restrict__ pxp = pairs;
     const float2 *__restrict__ pyp = pairs + V;
     const float2 *__restrict__ pzp = pairs + 2 * (size_t)V;
-    // Each component's four voxels differ from its base voxel by the steps
-    // M -> P along two axes (0 where the clamp merges them).
-    const uint32_t bx = voxel(g, xO, yM, zM), by = voxel(g, xM, yO, zM), bz = voxel(g, xM, yM, zO);
-    const uint32_t dx = (uint32_t)(xP - xM);
-    const uint32_t dy = (uint32_t)(yP - yM) * (uint32_t)g.nx;
-    const uint32_t dz = (uint32_t)(zP - zM) * ((uint32_t)g.nx * (uint32_t)g.ny);
-    const float2 x00 = __ldg(pxp + bx);
-    const float2 x10 = __ldg(pxp + bx + dy);
-    const float2 x01 = __ldg(pxp + bx + dz);
-    const float2 x11 = __ldg(pxp + bx + dy + dz);
-    const float2 yM0 = __ldg(pyp + by);
-    const float2 yP0 = __ldg(pyp + by + dx);
-    const float2 yM1 = __ldg(pyp + by + dz);
-    const float2 yP1 = __ldg(pyp + by + dx + dz);
-    const float2 zMM = __ldg(pzp + bz);
-    const float2 zMP = __ldg(pzp + bz + dy);
-    const float2 zPM = __ldg(pzp + bz + dx);
-    const float2 zPP = __ldg(pzp + bz + dx + dy);
+    const float2 x00 = __ldg(pxp + voxel(g, xO, yM, zM));
+    const float2 x10 = __ldg(pxp + voxel(g, xO, yP, zM));
+    const float2 x01 = __ldg(pxp + voxel(g, xO, yM, zP));
+    const float2 x11 = __ldg(pxp + voxel(g, xO, yP, zP));
+    const float2 yM0 = __ldg(pyp + voxel(g, xM, yO, zM));
+    const float2 yP0 = __ldg(pyp + voxel(g, xP, yO, zM));
+    const float2 yM1 = __ldg(pyp + voxel(g, xM, yO, zP));
+    const float2 yP1 = __ldg(pyp + voxel(g, xP, yO, zP));
+    const float2 zMM = __ldg(pzp + voxel(g, xM, yM, zO));
+    const float2 zMP = __ldg(pzp + voxel(g, xM, yP, zO));
+    const float2 zPM = __ldg(pzp + voxel(g, xP, yM, zO));
+    const float2 zPP = __ldg(pzp + voxel(g, xP, yP, zO));
     c.x00 = x00;
     c.dx10 = make_float2(x10.x - x00.x, x10.y - x00.y);
     c.x01 = x01;
@@ -199,15 +172,14 @@ __device__ __forceinline__ float3 interpolate(const CellCache &c, const float3 &
 }
 
 // Velocity at a position; `c` carries the last gathered cell, and the
-// samples are loaded again only when the position is not surely inside it.
+// samples are loaded again only when the position lies in another cell.
 __device__ __forceinline__ float3 velocity_cached(const GridDev &g, const float2 *__restrict__ pairs, float px,
                                                   float py, float pz, CellCache &c, bool &have)
 {
-    const bool inside = have && px >= c.lox && px < c.hix && py >= c.loy && py < c.hiy && pz >= c.loz &&
-                        pz < c.hiz;
-    if (!inside) {
-        int kx, ky, kz;
-        cell_key(g, px, py, pz, kx, ky, kz);
+    int kx, ky, kz;
+    const unsigned long long key = cell_key(g, px, py, pz, kx, ky, kz);
+    if (!have || key != c.key) {
+        c.key = key;
         gather_cell(g, pairs, kx, ky, kz, c);
         have = true;
     }

@@ -24,13 +24,7 @@ struct GridDev {
     float shift[3];  // aabb min + extent: the reference's index offset (psfsolver.cpp:80)
     uint32_t yoff;   // number of z-faces
     uint32_t xoff;   // number of z- and y-faces
-    float half_h;    // h / 2: width of a tracer cell (floor(2 gi) per axis)
-    float margin;    // CELL_MARGIN * h: by how much the tracer shrinks a cached cell
 };
-
-// Margin, in voxels, by which the tracer shrinks a cached cell's bounds
-// (see cell_bounds in psf_device.cuh).
-constexpr float CELL_MARGIN = 1e-3f;
 
 struct StateParams {
     double dt;
