@@ -137,24 +137,36 @@ psf::GridDev make_grid_dev(const psf_grid &g)
 using psf::fold_signs;
 using psf::n_faces_of;
 
-// A context keeps two coefficient buffers.  `vis` holds the state the caller
-// sees (w^n after n steps); the other holds w^{n+1}, already computed (the
-// contraction "primes" it whenever the state, the forcing or the parameters
-// change).  A step reconstructs and traces with w^{n+1} and, on a parallel
-// branch of the same graph, contracts w^{n+1} into w^{n+2} in the buffer it
-// leaves behind; then the buffers swap roles.  Each buffer carries its step
-// count, so the tracer reads the count of the buffer no kernel writes.
+// Software-pipelined step.  A context keeps three coefficient buffers (a ring)
+// and two face-pair / velocity buffers.  Between steps, with the caller's
+// state w^n in ring slot `vis` ("primed"): slot vis+1 holds w^{n+1}, slot
+// vis+2 holds w^{n+2}, and face set `tq` holds the face pairs and velocity
+// of w^{n+1}.  A step then runs, as three independent branches of one graph,
+//   the tracer with face set tq                          (step n's particles)
+//   the reconstruction of w^{n+2} into the other face set (step n+1's field)
+//   the contraction of w^{n+2} into w^{n+3}, in slot vis  (step n+2's state)
+// and the roles rotate.  Each kernel does one step's work of the reference's
+// phase order, so results are bit-identical to running the phases one after
+// the other.  Any change of state, forcing or parameters drops the lookahead
+// ("unprimed"); the next step is then a bootstrap graph: contraction ->
+// reconstruction -> tracer on the main branch and, beside it, the
+// contractions and the reconstruction that prime the pipeline again.  Every
+// ring slot carries its step count; the tracer reads the count of a slot no
+// kernel of the step writes.
 struct psf_ctx {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;   // the contraction's branch during graph capture
-    cudaEvent_t fork = nullptr, join = nullptr;
-    cudaGraph_t graphs[2] = {nullptr, nullptr};
-    cudaGraphExec_t execs[2] = {nullptr, nullptr};  // index: the buffer the step reconstructs from
-    double *wbuf[2] = {nullptr, nullptr};
-    unsigned long long *ctrbuf = nullptr;           // [2] completed steps of each buffer's state
-    int vis = 0;
+    cudaStream_t side[2] = {nullptr, nullptr};  // extra branches during graph capture
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr}, mid = nullptr, after_b = nullptr;
+    cudaGraph_t graphs[2][6] = {};              // [bootstrap, steady][vis * 2 + tq]
+    cudaGraphExec_t execs[2][6] = {};
+    double *wbuf[3] = {nullptr, nullptr, nullptr};
+    unsigned long long *ctrbuf = nullptr;       // [3] completed steps of each slot's state
+    float *ubuf[2] = {nullptr, nullptr};
+    float2 *pbuf[2] = {nullptr, nullptr};
+    int vis = 0, tq = 0;
+    bool primed = false;
     bool have_state = false;
     psf_grid grid{};
     psf_params params{};
@@ -168,28 +180,48 @@ struct psf_ctx {
     {
         drop_graph();
         for (void *p : allocs) cudaFree(p);
-        if (fork) cudaEventDestroy(fork);
-        if (join) cudaEventDestroy(join);
-        if (side) cudaStreamDestroy(side);
+        for (cudaEvent_t e : {fork, join[0], join[1], mid, after_b})
+            if (e) cudaEventDestroy(e);
+        for (cudaStream_t s : side)
+            if (s) cudaStreamDestroy(s);
         if (stream) cudaStreamDestroy(stream);
     }
     void drop_graph()
     {
-        for (int p = 0; p < 2; ++p) {
-            if (execs[p]) cudaGraphExecDestroy(execs[p]);
-            if (graphs[p]) cudaGraphDestroy(graphs[p]);
-            execs[p] = nullptr;
-            graphs[p] = nullptr;
-        }
+        for (int k = 0; k < 2; ++k)
+            for (int i = 0; i < 6; ++i) {
+                if (execs[k][i]) cudaGraphExecDestroy(execs[k][i]);
+                if (graphs[k][i]) cudaGraphDestroy(graphs[k][i]);
+                execs[k][i] = nullptr;
+                graphs[k][i] = nullptr;
+            }
     }
-    // Device view of a step that reconstructs from buffer p and contracts it into the other one.
-    psf::PlainDev dev_for(int p) const
+    int slot(int k) const { return (vis + k) % 3; }
+    // Contraction of ring slot `from` into `to`.
+    psf::PlainDev contraction(int from, int to) const
     {
         psf::PlainDev v = d;
-        v.w = wbuf[p];
-        v.w_next = wbuf[1 - p];
-        v.step_ctr = ctrbuf + p;
-        v.step_ctr_next = ctrbuf + (1 - p);
+        v.w = wbuf[from];
+        v.w_next = wbuf[to];
+        v.step_ctr = ctrbuf + from;
+        v.step_ctr_next = ctrbuf + to;
+        return v;
+    }
+    // Reconstruction of ring slot `from` into face set `fs`.
+    psf::PlainDev reconstruction(int from, int fs) const
+    {
+        psf::PlainDev v = d;
+        v.w = wbuf[from];
+        v.u = ubuf[fs];
+        v.pairs = pbuf[fs];
+        return v;
+    }
+    // Tracer with face set `fs`, keyed by the step count of ring slot `from`.
+    psf::PlainDev tracer(int from, int fs) const
+    {
+        psf::PlainDev v = d;
+        v.trace_pairs = pbuf[fs];
+        v.trace_ctr = ctrbuf + from;
         return v;
     }
     template <class T>
@@ -223,12 +255,6 @@ struct psf_ctx {
         if (e_ != cudaSuccess) return psf::cuda_fail(e_, #x); \
     } while (0)
 
-// w^{n+1} from the visible w^n into the other buffer (stream-ordered).
-static int prime(psf_ctx *c)
-{
-    return psf::launch_contract_state(c->dev_for(c->vis), c->stream);
-}
-
 static int apply_params(psf_ctx *c, const psf_params &p)
 {
     if (!(p.timestep > 0.0) || !std::isfinite(p.timestep))
@@ -246,11 +272,7 @@ static int apply_params(psf_ctx *c, const psf_params &p)
     c->d.tp.rk4 = p.integrator == PSF_RK4;
     c->d.tp.seed = p.seed;
     c->drop_graph();
-    if (c->have_state) {
-        PSF_CHECK(prime(c));
-        cudaError_t e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) return psf::cuda_fail(e, "priming the next state");
-    }
+    c->primed = false;
     return PSF_OK;
 }
 
@@ -261,34 +283,71 @@ static int sync_stream(psf_ctx *c)
     return PSF_OK;
 }
 
-// One step as a graph: reconstruction -> tracer on the context's stream,
-// and beside them the next step's contraction on a forked branch.
-static int build_graph(psf_ctx *c, int p)
+// Capture one step into a graph.  `boot`: the pipeline is not primed (only
+// the caller's state in slot vis is valid).
+static int capture_step(psf_ctx *c, bool boot, cudaGraph_t *out)
 {
-    if (c->execs[p]) return PSF_OK;
-    const psf::PlainDev dp = c->dev_for(p);
-    PSF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int v0 = c->slot(0), v1 = c->slot(1), v2 = c->slot(2);
+    const int q = c->tq;
+    cudaStream_t m = c->stream, s0 = c->side[0], s1 = c->side[1];
     int rc = PSF_OK;
-    cudaError_t e = cudaEventRecord(c->fork, c->stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->fork, 0);
-    if (e != cudaSuccess) rc = psf::cuda_fail(e, "forking the contraction branch");
-    if (rc == PSF_OK) rc = psf::launch_contract_state(dp, c->side);
-    if (rc == PSF_OK) rc = psf::launch_reconstruct(dp, c->stream, /*after_kernel=*/false);
-    if (rc == PSF_OK) rc = psf::launch_trace(dp, c->stream);
+    auto ok = [&](cudaError_t e, const char *what) {
+        if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, what);
+        return rc == PSF_OK;
+    };
+    if (!ok(cudaStreamBeginCapture(m, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")) return rc;
+    if (boot) {
+        // main: w^{n+1}, its field, step n's particles; beside it: w^{n+2}, its field, w^{n+3}.
+        rc = psf::launch_contract_state(c->contraction(v0, v1), m);
+        if (ok(cudaEventRecord(c->mid, m), "fork") && ok(cudaStreamWaitEvent(s0, c->mid, 0), "fork")) {
+            rc = psf::launch_contract_state(c->contraction(v1, v2), s0);
+            if (rc == PSF_OK && ok(cudaEventRecord(c->after_b, s0), "fork") &&
+                ok(cudaStreamWaitEvent(s1, c->after_b, 0), "fork"))
+                rc = psf::launch_reconstruct(c->reconstruction(v2, 1 - q), s1, /*after_kernel=*/false);
+            if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(v2, v0), s0);
+        }
+        if (rc == PSF_OK) rc = psf::launch_reconstruct(c->reconstruction(v1, q), m, /*after_kernel=*/false);
+        if (rc == PSF_OK) rc = psf::launch_trace(c->tracer(v1, q), m, /*after_kernel=*/true);
+    } else {
+        // step n's particles, step n+1's field, step n+2's state: three independent branches.
+        if (ok(cudaEventRecord(c->fork, m), "fork") && ok(cudaStreamWaitEvent(s0, c->fork, 0), "fork") &&
+            ok(cudaStreamWaitEvent(s1, c->fork, 0), "fork")) {
+            rc = psf::launch_reconstruct(c->reconstruction(v2, 1 - q), s0, /*after_kernel=*/false);
+            if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(v2, v0), s1);
+            if (rc == PSF_OK) rc = psf::launch_trace(c->tracer(v1, q), m, /*after_kernel=*/false);
+        }
+    }
     if (rc == PSF_OK) {
-        e = cudaEventRecord(c->join, c->side);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->join, 0);
-        if (e != cudaSuccess) rc = psf::cuda_fail(e, "joining the contraction branch");
+        ok(cudaEventRecord(c->join[0], s0), "join") && ok(cudaStreamWaitEvent(m, c->join[0], 0), "join") &&
+            ok(cudaEventRecord(c->join[1], s1), "join") && ok(cudaStreamWaitEvent(m, c->join[1], 0), "join");
     }
     cudaGraph_t g = nullptr;
-    e = cudaStreamEndCapture(c->stream, &g);
+    cudaError_t e = cudaStreamEndCapture(m, &g);
     if (rc != PSF_OK) {
         if (g) cudaGraphDestroy(g);
         return rc;
     }
     if (e != cudaSuccess) return psf::cuda_fail(e, "cudaStreamEndCapture");
-    c->graphs[p] = g;
-    PSF_CUDA(cudaGraphInstantiate(&c->execs[p], g, 0));
+    *out = g;
+    return PSF_OK;
+}
+
+// Launch one step (bootstrap or steady graph for the current ring position)
+// and rotate the ring.
+static int launch_step(psf_ctx *c)
+{
+    const int kind = c->primed ? 1 : 0;
+    const int idx = c->vis * 2 + c->tq;
+    if (!c->execs[kind][idx]) {
+        cudaGraph_t g = nullptr;
+        PSF_CHECK(capture_step(c, kind == 0, &g));
+        c->graphs[kind][idx] = g;
+        PSF_CUDA(cudaGraphInstantiate(&c->execs[kind][idx], g, 0));
+    }
+    PSF_CUDA(cudaGraphLaunch(c->execs[kind][idx], c->stream));
+    c->vis = c->slot(1);
+    c->tq = 1 - c->tq;
+    c->primed = true;
     return PSF_OK;
 }
 
@@ -363,9 +422,10 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaSetDevice"));
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
+    for (cudaStream_t *s : {&c->side[0], &c->side[1]})
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+    for (cudaEvent_t *ev : {&c->fork, &c->join[0], &c->join[1], &c->mid, &c->after_b})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaStreamCreate"));
     c->grid = g;
     if ((rc = fold_signs(g, b->sign_bits, c->sigma)) != PSF_OK) return bail(rc);
@@ -398,19 +458,22 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         int32_t *faces = nullptr;
         double *lam = nullptr, *force = nullptr;
         if ((rc = c->alloc(&C, hC.size())) || (rc = c->alloc(&phiT, hP.size())) ||
-            (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&c->wbuf[0], 2 * (size_t)N)) ||
+            (rc = c->alloc(&faces, (size_t)b->n_active)) || (rc = c->alloc(&c->wbuf[0], 3 * (size_t)N)) ||
             (rc = c->alloc(&d.dwpart, (size_t)N * d.S)) || (rc = c->alloc(&lam, (size_t)N)) ||
             (rc = c->alloc(&force, (size_t)N)) || (rc = c->alloc(&d.ticket, 1)) ||
-            (rc = c->alloc(&c->ctrbuf, 2)) || (rc = c->alloc(&d.u, (size_t)F)))
+            (rc = c->alloc(&c->ctrbuf, 3)) || (rc = c->alloc(&c->ubuf[0], 2 * (size_t)F)))
             return bail(rc);
         c->wbuf[1] = c->wbuf[0] + N;
+        c->wbuf[2] = c->wbuf[0] + 2 * N;
+        c->ubuf[1] = c->ubuf[0] + F;
         // Per-voxel face pairs read by the tracer, and where each active face goes.
         std::vector<int32_t> hdst;
         psf::face_pair_slots(g, b->active_faces, b->n_active, hdst);
         int32_t *pdst = nullptr;
-        if ((rc = c->alloc(&d.pairs, (size_t)(3 * V))) || (rc = c->alloc(&pdst, hdst.size()))) return bail(rc);
+        if ((rc = c->alloc(&c->pbuf[0], (size_t)(6 * V))) || (rc = c->alloc(&pdst, hdst.size()))) return bail(rc);
+        c->pbuf[1] = c->pbuf[0] + 3 * V;
         d.pair_dst = pdst;
-        if ((e = cudaMemsetAsync(d.pairs, 0, (size_t)(3 * V) * sizeof(float2), c->stream)) ||
+        if ((e = cudaMemsetAsync(c->pbuf[0], 0, (size_t)(6 * V) * sizeof(float2), c->stream)) ||
             (e = cudaMemcpyAsync(pdst, hdst.data(), hdst.size() * 4, cudaMemcpyHostToDevice, c->stream)) ||
             (e = cudaStreamSynchronize(c->stream)))
             return bail(psf::cuda_fail(e, "face pair upload"));
@@ -425,9 +488,9 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
             (e = cudaMemcpyAsync(faces, b->active_faces, (size_t)b->n_active * 4, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(lam, b->eigenvalues, (size_t)N * 8, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemsetAsync(force, 0, (size_t)N * 8, st)) ||
-            (e = cudaMemsetAsync(c->wbuf[0], 0, 2 * (size_t)N * 8, st)) ||
-            (e = cudaMemsetAsync(d.ticket, 0, 4, st)) || (e = cudaMemsetAsync(c->ctrbuf, 0, 16, st)) ||
-            (e = cudaMemsetAsync(d.u, 0, (size_t)F * 4, st)) || (e = cudaStreamSynchronize(st)))
+            (e = cudaMemsetAsync(c->wbuf[0], 0, 3 * (size_t)N * 8, st)) ||
+            (e = cudaMemsetAsync(d.ticket, 0, 4, st)) || (e = cudaMemsetAsync(c->ctrbuf, 0, 24, st)) ||
+            (e = cudaMemsetAsync(c->ubuf[0], 0, 2 * (size_t)F * 4, st)) || (e = cudaStreamSynchronize(st)))
             return bail(psf::cuda_fail(e, "basis upload"));
     } catch (const std::bad_alloc &) {
         return bail(fail(PSF_ERR_NOMEM, "host staging allocation failed"));
@@ -463,8 +526,8 @@ int psf_set_state(psf_ctx *c, const double *w, int32_t n)
     if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
     PSF_CUDA(cudaSetDevice(c->device));
     PSF_CUDA(cudaMemcpyAsync(c->wbuf[c->vis], w, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
-    PSF_CHECK(prime(c));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
+    c->primed = false;
     c->have_state = true;
     return PSF_OK;
 }
@@ -486,8 +549,8 @@ int psf_set_forcing(psf_ctx *c, const double *f, int32_t n)
     PSF_CUDA(cudaSetDevice(c->device));
     PSF_CUDA(cudaMemcpyAsync(const_cast<double *>(c->d.force), f, (size_t)n * 8, cudaMemcpyHostToDevice,
                              c->stream));
-    if (c->have_state) PSF_CHECK(prime(c));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
+    c->primed = false;
     return PSF_OK;
 }
 
@@ -550,7 +613,7 @@ int psf_get_velocity(psf_ctx *c, float *u, int64_t n_faces)
     if (!c || !u) return fail(PSF_ERR_INVALID, "null argument");
     if (n_faces != c->d.n_faces) return fail(PSF_ERR_INVALID, "n_faces must equal the grid's face count");
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CUDA(cudaMemcpyAsync(u, c->d.u, (size_t)n_faces * 4, cudaMemcpyDeviceToHost, c->stream));
+    PSF_CUDA(cudaMemcpyAsync(u, c->ubuf[1 - c->tq], (size_t)n_faces * 4, cudaMemcpyDeviceToHost, c->stream));
     PSF_CHECK(sync_stream(c));
     for (int64_t f = 0; f < n_faces; ++f) u[f] *= (float)c->sigma[(size_t)f];
     return PSF_OK;
@@ -562,13 +625,7 @@ int psf_step(psf_ctx *c, int32_t nsteps)
     if (nsteps < 0) return fail(PSF_ERR_INVALID, "nsteps must be >= 0");
     if (!c->have_state) return fail(PSF_ERR_STATE, "psf_set_state must be called before stepping");
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CHECK(build_graph(c, 0));
-    PSF_CHECK(build_graph(c, 1));
-    for (int32_t i = 0; i < nsteps; ++i) {
-        const int p = 1 - c->vis;  // the buffer holding w^{n+1}
-        PSF_CUDA(cudaGraphLaunch(c->execs[p], c->stream));
-        c->vis = p;
-    }
+    for (int32_t i = 0; i < nsteps; ++i) PSF_CHECK(launch_step(c));
     return PSF_OK;
 }
 
@@ -604,20 +661,28 @@ int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
     for (int i = 0; i <= nk; ++i) PSF_CUDA(cudaEventCreate(&ev[i]));
     int rc = PSF_OK;
     cudaStream_t st = c->stream;
-    // The kernels of one step, one after the other: the contraction of the
-    // next state, then the reconstruction and the tracer of this one.
-    const int p = 1 - c->vis;
-    const psf::PlainDev dp = c->dev_for(p);
+    // The kernels of one (steady) step, one after the other: the contraction
+    // of w^{n+3}, the reconstruction of w^{n+2}, the tracer of step n.  An
+    // unprimed pipeline is primed first, untimed.
+    if (!c->primed) {
+        rc = psf::launch_contract_state(c->contraction(c->slot(0), c->slot(1)), st);
+        if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(c->slot(1), c->slot(2)), st);
+        if (rc == PSF_OK) rc = psf::launch_reconstruct(c->reconstruction(c->slot(1), c->tq), st, false);
+        if (rc == PSF_OK) c->primed = true;
+    }
     cudaEventRecord(ev[0], st);
-    if (rc == PSF_OK) rc = psf::launch_contract_state(dp, st);
+    if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(c->slot(2), c->slot(0)), st);
     cudaEventRecord(ev[1], st);
-    if (rc == PSF_OK) rc = psf::launch_reconstruct(dp, st, /*after_kernel=*/false);
+    if (rc == PSF_OK) rc = psf::launch_reconstruct(c->reconstruction(c->slot(2), 1 - c->tq), st, false);
     cudaEventRecord(ev[2], st);
     if (rc == PSF_OK && nk == 3) {
-        rc = psf::launch_trace(dp, st);
+        rc = psf::launch_trace(c->tracer(c->slot(1), c->tq), st, false);
         cudaEventRecord(ev[3], st);
     }
-    if (rc == PSF_OK) c->vis = p;
+    if (rc == PSF_OK) {
+        c->vis = c->slot(1);
+        c->tq = 1 - c->tq;
+    }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");
     for (int i = 0; rc == PSF_OK && i < nk; ++i) {

@@ -291,8 +291,8 @@ __global__ void __launch_bounds__(256) psf_reconstruct(const float *__restrict__
 // Persistent grid (a whole number of resident blocks per SM) striding over
 // the particles, which are stored in cell order.  A thread's first particle
 // is loaded before the grid-dependency wait: the particles were last written
-// by the previous step's tracer, which completed before this step's
-// contraction passed its own wait.
+// by the previous step's tracer, which belongs to an earlier graph launch
+// (or an earlier, synchronised profiling step).
 constexpr int TRACE_THREADS = 256;
 
 __global__ void __launch_bounds__(TRACE_THREADS, 3) psf_trace(float4 *__restrict__ parts, long long P,
@@ -439,15 +439,15 @@ int trace_blocks_per_sm()
     return per_sm;
 }
 
-int launch_trace(const PlainDev &d, cudaStream_t st)
+int launch_trace(const PlainDev &d, cudaStream_t st, bool after_kernel)
 {
     if (d.P == 0) return PSF_OK;
     const long long blocks =
         std::min<long long>((d.P + TRACE_THREADS - 1) / TRACE_THREADS, std::max(1, d.trace_blocks));
     PdlLaunch L((unsigned)blocks, TRACE_THREADS, st);
+    if (!after_kernel) L.cfg.numAttrs = 0;
     cudaError_t e = cudaLaunchKernelEx(&L.cfg, psf_trace, d.parts, (long long)d.P, (const int32_t *)d.perm,
-                                       (const float2 *)d.pairs, d.grid, d.tp,
-                                       (const unsigned long long *)d.step_ctr);
+                                       d.trace_pairs, d.grid, d.tp, d.trace_ctr);
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "psf_trace launch");
 }
 

@@ -56,7 +56,9 @@ struct PlainDev {
     unsigned int *ticket;
     unsigned long long *step_ctr, *step_ctr_next;
     float *u;            // [n_faces], signed
-    float2 *pairs;       // [3][V] per-voxel face pairs (x, y, z), signed
+    float2 *pairs;       // [3][V] per-voxel face pairs (x, y, z), signed: written by the reconstruction
+    const float2 *trace_pairs;                // the face pairs the tracer reads
+    const unsigned long long *trace_ctr;      // step count of the state the tracer advects with
     const int32_t *pair_dst;  // [n_active][2] float indices into pairs of each active face
     int trace_blocks;    // persistent tracer grid: SMs x resident blocks per SM
     float4 *parts;       // [P] in cell (Morton) order
@@ -106,7 +108,7 @@ int launch_contract_state(const PlainDev &d, cudaStream_t st);
 // `after_kernel`: the launch directly follows a kernel in the stream and may
 // start during that kernel's tail (programmatic dependent launch).
 int launch_reconstruct(const PlainDev &d, cudaStream_t st, bool after_kernel = true);
-int launch_trace(const PlainDev &d, cudaStream_t st);
+int launch_trace(const PlainDev &d, cudaStream_t st, bool after_kernel = true);
 int trace_blocks_per_sm();
 int sort_particles_temp_bytes(long long P, size_t *bytes);
 int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);
