@@ -148,25 +148,29 @@ using psf::n_faces_of;
 // and the roles rotate.  Each kernel does one step's work of the reference's
 // phase order, so results are bit-identical to running the phases one after
 // the other.  Any change of state, forcing or parameters drops the lookahead
-// ("unprimed"); the next step is then a bootstrap graph: contraction ->
-// reconstruction -> tracer on the main branch and, beside it, the
-// contractions and the reconstruction that prime the pipeline again.  Every
-// ring slot carries its step count; the tracer reads the count of a slot no
-// kernel of the step writes.
+// ("unprimed").  The first step after such a change is a lean graph
+// (contraction -> reconstruction -> tracer, nothing ahead), so a caller that
+// resets the state before every step pays for no lookahead; a step taken
+// while unprimed but with no change since the previous step is a bootstrap
+// graph: the lean chain on the main branch and, beside it, the contractions
+// and the reconstruction that prime the pipeline.  Every ring slot carries
+// its step count; the tracer reads the count of a slot no kernel of the step
+// writes.
 struct psf_ctx {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     cudaStream_t side[2] = {nullptr, nullptr};  // extra branches during graph capture
     cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr}, mid = nullptr, after_b = nullptr;
-    cudaGraph_t graphs[2][6] = {};              // [bootstrap, steady][vis * 2 + tq]
-    cudaGraphExec_t execs[2][6] = {};
+    cudaGraph_t graphs[3][6] = {};              // [lean, bootstrap, steady][vis * 2 + tq]
+    cudaGraphExec_t execs[3][6] = {};
     double *wbuf[3] = {nullptr, nullptr, nullptr};
     unsigned long long *ctrbuf = nullptr;       // [3] completed steps of each slot's state
     float *ubuf[2] = {nullptr, nullptr};
     float2 *pbuf[2] = {nullptr, nullptr};
     int vis = 0, tq = 0;
     bool primed = false;
+    bool changed = true;  // a setter ran since the last step
     bool have_state = false;
     psf_grid grid{};
     psf_params params{};
@@ -188,7 +192,7 @@ struct psf_ctx {
     }
     void drop_graph()
     {
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < 3; ++k)
             for (int i = 0; i < 6; ++i) {
                 if (execs[k][i]) cudaGraphExecDestroy(execs[k][i]);
                 if (graphs[k][i]) cudaGraphDestroy(graphs[k][i]);
@@ -197,6 +201,7 @@ struct psf_ctx {
             }
     }
     int slot(int k) const { return (vis + k) % 3; }
+    static int slot_of(int v, int k) { return (v + k) % 3; }
     // Contraction of ring slot `from` into `to`.
     psf::PlainDev contraction(int from, int to) const
     {
@@ -273,6 +278,7 @@ static int apply_params(psf_ctx *c, const psf_params &p)
     c->d.tp.seed = p.seed;
     c->drop_graph();
     c->primed = false;
+    c->changed = true;
     return PSF_OK;
 }
 
@@ -283,12 +289,12 @@ static int sync_stream(psf_ctx *c)
     return PSF_OK;
 }
 
-// Capture one step into a graph.  `boot`: the pipeline is not primed (only
-// the caller's state in slot vis is valid).
-static int capture_step(psf_ctx *c, bool boot, cudaGraph_t *out)
+enum StepKind { STEP_LEAN = 0, STEP_BOOT = 1, STEP_STEADY = 2 };
+
+// Capture one step of the given kind, for ring position (v, q), into a graph.
+static int capture_step(psf_ctx *c, int kind, int v, int q, cudaGraph_t *out)
 {
-    const int v0 = c->slot(0), v1 = c->slot(1), v2 = c->slot(2);
-    const int q = c->tq;
+    const int v0 = psf_ctx::slot_of(v, 0), v1 = psf_ctx::slot_of(v, 1), v2 = psf_ctx::slot_of(v, 2);
     cudaStream_t m = c->stream, s0 = c->side[0], s1 = c->side[1];
     int rc = PSF_OK;
     auto ok = [&](cudaError_t e, const char *what) {
@@ -296,28 +302,34 @@ static int capture_step(psf_ctx *c, bool boot, cudaGraph_t *out)
         return rc == PSF_OK;
     };
     if (!ok(cudaStreamBeginCapture(m, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")) return rc;
-    if (boot) {
-        // main: w^{n+1}, its field, step n's particles; beside it: w^{n+2}, its field, w^{n+3}.
-        rc = psf::launch_contract_state(c->contraction(v0, v1), m);
-        if (ok(cudaEventRecord(c->mid, m), "fork") && ok(cudaStreamWaitEvent(s0, c->mid, 0), "fork")) {
-            rc = psf::launch_contract_state(c->contraction(v1, v2), s0);
-            if (rc == PSF_OK && ok(cudaEventRecord(c->after_b, s0), "fork") &&
-                ok(cudaStreamWaitEvent(s1, c->after_b, 0), "fork"))
-                rc = psf::launch_reconstruct(c->reconstruction(v2, 1 - q), s1, /*after_kernel=*/false);
-            if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(v2, v0), s0);
-        }
-        if (rc == PSF_OK) rc = psf::launch_reconstruct(c->reconstruction(v1, q), m, /*after_kernel=*/false);
-        if (rc == PSF_OK) rc = psf::launch_trace(c->tracer(v1, q), m, /*after_kernel=*/true);
-    } else {
+    bool forked = false;
+    if (kind == STEP_STEADY) {
         // step n's particles, step n+1's field, step n+2's state: three independent branches.
-        if (ok(cudaEventRecord(c->fork, m), "fork") && ok(cudaStreamWaitEvent(s0, c->fork, 0), "fork") &&
-            ok(cudaStreamWaitEvent(s1, c->fork, 0), "fork")) {
+        forked = ok(cudaEventRecord(c->fork, m), "fork") && ok(cudaStreamWaitEvent(s0, c->fork, 0), "fork") &&
+                 ok(cudaStreamWaitEvent(s1, c->fork, 0), "fork");
+        if (forked) {
             rc = psf::launch_reconstruct(c->reconstruction(v2, 1 - q), s0, /*after_kernel=*/false);
             if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(v2, v0), s1);
             if (rc == PSF_OK) rc = psf::launch_trace(c->tracer(v1, q), m, /*after_kernel=*/false);
         }
+    } else {
+        // main: w^{n+1}, its field, step n's particles.
+        rc = psf::launch_contract_state(c->contraction(v0, v1), m);
+        if (rc == PSF_OK && kind == STEP_BOOT) {
+            // beside it: w^{n+2}, its field, w^{n+3}.
+            forked = ok(cudaEventRecord(c->mid, m), "fork") && ok(cudaStreamWaitEvent(s0, c->mid, 0), "fork");
+            if (forked) {
+                rc = psf::launch_contract_state(c->contraction(v1, v2), s0);
+                if (rc == PSF_OK && ok(cudaEventRecord(c->after_b, s0), "fork") &&
+                    ok(cudaStreamWaitEvent(s1, c->after_b, 0), "fork"))
+                    rc = psf::launch_reconstruct(c->reconstruction(v2, 1 - q), s1, /*after_kernel=*/false);
+                if (rc == PSF_OK) rc = psf::launch_contract_state(c->contraction(v2, v0), s0);
+            }
+        }
+        if (rc == PSF_OK) rc = psf::launch_reconstruct(c->reconstruction(v1, q), m, /*after_kernel=*/true);
+        if (rc == PSF_OK) rc = psf::launch_trace(c->tracer(v1, q), m, /*after_kernel=*/true);
     }
-    if (rc == PSF_OK) {
+    if (rc == PSF_OK && forked) {
         ok(cudaEventRecord(c->join[0], s0), "join") && ok(cudaStreamWaitEvent(m, c->join[0], 0), "join") &&
             ok(cudaEventRecord(c->join[1], s1), "join") && ok(cudaStreamWaitEvent(m, c->join[1], 0), "join");
     }
@@ -332,22 +344,28 @@ static int capture_step(psf_ctx *c, bool boot, cudaGraph_t *out)
     return PSF_OK;
 }
 
-// Launch one step (bootstrap or steady graph for the current ring position)
-// and rotate the ring.
+// Launch one step and rotate the ring.  The six ring positions of a step
+// kind are captured together, the first time that kind is needed.
 static int launch_step(psf_ctx *c)
 {
-    const int kind = c->primed ? 1 : 0;
+    const int kind = c->primed ? STEP_STEADY : (c->changed ? STEP_LEAN : STEP_BOOT);
     const int idx = c->vis * 2 + c->tq;
     if (!c->execs[kind][idx]) {
-        cudaGraph_t g = nullptr;
-        PSF_CHECK(capture_step(c, kind == 0, &g));
-        c->graphs[kind][idx] = g;
-        PSF_CUDA(cudaGraphInstantiate(&c->execs[kind][idx], g, 0));
+        for (int v = 0; v < 3; ++v)
+            for (int q = 0; q < 2; ++q) {
+                const int i = v * 2 + q;
+                if (c->execs[kind][i]) continue;
+                cudaGraph_t g = nullptr;
+                PSF_CHECK(capture_step(c, kind, v, q, &g));
+                c->graphs[kind][i] = g;
+                PSF_CUDA(cudaGraphInstantiate(&c->execs[kind][i], g, 0));
+            }
     }
     PSF_CUDA(cudaGraphLaunch(c->execs[kind][idx], c->stream));
     c->vis = c->slot(1);
     c->tq = 1 - c->tq;
-    c->primed = true;
+    c->primed = kind != STEP_LEAN;
+    c->changed = false;
     return PSF_OK;
 }
 
@@ -528,6 +546,7 @@ int psf_set_state(psf_ctx *c, const double *w, int32_t n)
     PSF_CUDA(cudaMemcpyAsync(c->wbuf[c->vis], w, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
     c->primed = false;
+    c->changed = true;
     c->have_state = true;
     return PSF_OK;
 }
@@ -551,6 +570,7 @@ int psf_set_forcing(psf_ctx *c, const double *f, int32_t n)
                              c->stream));
     PSF_CUDA(cudaStreamSynchronize(c->stream));
     c->primed = false;
+    c->changed = true;
     return PSF_OK;
 }
 
@@ -682,6 +702,7 @@ int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
     if (rc == PSF_OK) {
         c->vis = c->slot(1);
         c->tq = 1 - c->tq;
+        c->changed = false;
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");

@@ -348,3 +348,41 @@ def build_basis(dom: Domain, n_modes: int, device=0, **kw):
     b = Basis(dom.dims, dom.h, dom.aabb_min, dom.aabb_max, dom.interior_faces.astype(np.int32), lam, grav, phi_I,
               C, dom.sign_bits, dom.inside.ravel().astype(np.uint8), name=dom.name)
     return b, stats
+
+
+def main(argv=None) -> None:
+    """Build one domain's basis on the GPU and print its statistics (optionally save it).
+
+    ``python -m parallelspectralfluids3d_b200.precompute box 24 128``
+    ``python -m parallelspectralfluids3d_b200.precompute sphere 40 384 --radius 10 --out b.psfb``
+    """
+    import argparse
+    import json
+
+    from .domain import box_domain, channel_domain, sphere_obstacle_domain
+
+    ap = argparse.ArgumentParser(description=main.__doc__.splitlines()[0])
+    ap.add_argument("kind", choices=["box", "sphere", "channel"])
+    ap.add_argument("dims", help="n or nx,ny,nz voxels")
+    ap.add_argument("modes", type=int)
+    ap.add_argument("--radius", type=float, default=None, help="sphere obstacle radius in voxels")
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default=None, help="write the basis here (.psfb)")
+    a = ap.parse_args(argv)
+    dims = tuple(int(x) for x in a.dims.split(","))
+    dims = dims[0] if len(dims) == 1 else dims
+    if a.kind == "sphere":
+        dom = sphere_obstacle_domain(dims, a.radius if a.radius is not None else 0.25 * min(np.atleast_1d(dims)))
+    elif a.kind == "channel":
+        dom = channel_domain(dims if isinstance(dims, tuple) else (dims,) * 3)
+    else:
+        dom = box_domain(dims)
+    b, stats = build_basis(dom, a.modes, device=a.device)
+    if a.out:
+        b.save(a.out)
+    print(json.dumps({"domain": dom.name, "modes": a.modes,
+                      **{k: (float(v) if isinstance(v, (float, np.floating)) else v) for k, v in stats.items()}}))
+
+
+if __name__ == "__main__":
+    main()

@@ -169,3 +169,24 @@ def test_changes_between_steps_take_effect_at_the_next_step(small_bases):
     assert rel_err(got_a, ref.w) <= W_TOL
     ref_b = O.OracleRollout(b, w1, None, dt=0.05, forcing=f, reconstruct=False).step(4)
     assert rel_err(got_b, ref_b.w) <= W_TOL
+
+
+def test_lean_bootstrap_and_steady_steps_agree(small_bases):
+    """Re-setting the state before every step (each step then runs the lean graph) gives the
+    same states, particles and velocity field as stepping on (bootstrap, then steady graphs)."""
+    b = small_bases["sphere12x10x9"]
+    w0 = initial_coefficients(b.n_modes, 8)
+    parts = initial_particles(b, 500, 8)
+    outs = []
+    for reset in (False, True):
+        ctx = Context(b, L.make_params(dt=0.03))
+        ctx.set_state(w0)
+        ctx.set_particles(parts)
+        for _ in range(9):
+            if reset:
+                ctx.set_state(ctx.get_state())
+            ctx.step(1)
+        outs.append((ctx.get_state(), ctx.get_particles(), ctx.get_velocity()))
+        ctx.close()
+    for a, c in zip(outs[0], outs[1]):
+        assert np.array_equal(a, c)
