@@ -420,7 +420,7 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------ batched arm
-def load_batch_workload(name, device):
+def load_batch_workload(name, device, particles=None):
     """Bases and per-instance inputs of a batched workload (seeded, synthetic)."""
     from parallelspectralfluids3d_b200.fixture import cached_basis, initial_coefficients, initial_particles
 
@@ -440,7 +440,8 @@ def load_batch_workload(name, device):
         insts.append(dict(basis=g, slot=i // len(bases), n=n, w0=w0, force=f, seed_p=wl["seed_p"](i)))
     slots = [sum(1 for x in insts if x["basis"] == g) for g in range(len(bases))]
     for x in insts:
-        x["parts"] = initial_particles(bases[x["basis"]], wl["particles"], x["seed_p"])
+        x["parts"] = initial_particles(bases[x["basis"]], wl["particles"] if particles is None else particles,
+                                       x["seed_p"])
     return wl, bases, slots, insts
 
 
@@ -931,14 +932,16 @@ def run_for_profiler(args):
     if args.workload in BATCH_WORKLOADS:
         from parallelspectralfluids3d_b200.batch import Batch
 
-        wl, bases, slots, insts = load_batch_workload(args.workload, "cuda")
+        wl, bases, slots, insts = load_batch_workload(args.workload, "cuda",
+                                                      particles=args.ncu_particles or None)
         if args.ncu_instances:
             insts = insts[: args.ncu_instances]
-            slots = [max(1, sum(1 for x in insts if x["basis"] == g)) for g in range(len(bases))]
-        batch = Batch(bases, slots=slots, max_particles=wl["particles"], autotune=False)
+            slots = assign_slots(insts, len(bases))
+        batch = Batch(bases, slots=slots, max_particles=max(len(x["parts"]) for x in insts), autotune=False)
         fill_batch(batch, wl, insts)
         for _ in range(args.ncu):
-            ms = batch.profile_step()
+            # --ncu-phases: contraction, state update, reconstruction and tracer as separate launches.
+            ms = batch.profile_phases() if args.ncu_phases else batch.profile_step()
         torch.cuda.synchronize()
         print(json.dumps({"profiled_steps": args.ncu, "batch": batch.info(),
                           "last_step_kernel_ms": [round(float(m), 5) for m in ms]}))
@@ -1073,6 +1076,9 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched tensor-core form in the default line")
     ap.add_argument("--batch-steps", type=int, default=50, help="timed steps of a batched workload")
     ap.add_argument("--ncu-instances", type=int, default=0, help="profiling driver: only the first K instances")
+    ap.add_argument("--ncu-particles", type=int, default=0, help="profiling driver: particles per instance")
+    ap.add_argument("--ncu-phases", action="store_true",
+                    help="profiling driver: run the batched phases as separate launches")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving: length of the arrival window")
     ap.add_argument("--serve-slots", type=int, default=96, help="serving: concurrent rollouts per domain")
     ap.add_argument("--serve-pool", type=int, default=64_000_000, help="serving: particles resident at once")
