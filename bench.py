@@ -62,6 +62,12 @@ BATCH_WORKLOADS = {
         particles=1 << 20, dt=0.005, force0=0.0, integrator=4, seed_w=lambda i: 100 + i,
         seed_p=lambda i: 10100 + i, full_steps=1000, check=[0, 31, 63], check_particles=[0, 31, 63],
         describe="48^3 channel, N=256 (C, Phi as BF16 hi+lo), 64 trajectories x 1M particles, RK4, dt=0.005"),
+    # The serving configuration's largest tile shape: 64 instances of N=384 on one 384-mode basis.
+    "channel64_n384_b64_p16384": dict(
+        bases=[(("channel", (64, 32, 32), None), 384)], instances=64, n_modes=lambda i, rng: 384,
+        particles=16384, dt=0.005, force0=0.0, integrator=4, seed_w=lambda i: 300 + i, seed_p=lambda i: 400 + i,
+        full_steps=500, check=[0, 63], check_particles=[0],
+        describe="64 instances of N=384 on the 64x32x32 channel, 16384 particles each, RK4, dt=0.005"),
     # Batching form: 512 instances, N ~ U{32..256}, domains in rotation, 16384 particles each.
     "mixed512_p16384": dict(
         bases=[(("box", 32, None), 256), (("sphere", 40, 10.0), 256), (("channel", (64, 32, 32), None), 256)],
