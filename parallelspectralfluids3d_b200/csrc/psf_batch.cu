@@ -398,14 +398,21 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             const Unit un = decode_unit(G, lt);
             const int outer = un.outer, inner = un.inner;
             // Contraction: the state values of this warp's rows for the first
-            // 32 slots are loaded while the accumulator is still being computed.
-            float wv[32];
+            // 64 slots are loaded while the accumulator is still being computed,
+            // and every later 32-slot chunk two chunks ahead of its use.
+            float wa[32], wb[32];
             const int a_row = inner * 128 + row;
             const bool arow = !recon && a_row < G.n_rows;
-            if (!recon) {
+            auto load_w = [&](float(&dst)[32], int c0) {
 #pragma unroll
-                for (int c = 0; c < 32; ++c)
-                    wv[c] = (arow && c < G.cap) ? G.wf[(size_t)c * G.ldw + a_row] : 0.f;
+                for (int c = 0; c < 32; ++c) {
+                    const int b = c0 + c;
+                    dst[c] = (arow && b < G.cap) ? G.wf[(size_t)b * G.ldw + a_row] : 0.f;
+                }
+            };
+            if (!recon) {
+                load_w(wa, 0);
+                if (32 < G.bn) load_w(wb, 32);
             }
             bool ok = mbar_wait(&acc_full[abuf], aphase, err, ERR_WAIT_ACC_FULL);
             ok = __all_sync(0xffffffffu, ok);
@@ -415,23 +422,21 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
             if (!recon) {
                 // dw partial of mode k = outer over this warp's 32 rows a:
                 // sum_a w[a][b] Y[a][b] for every slot b, in FP32.
-                for (int c0 = 0; c0 < G.bn; c0 += 32) {
+                auto chunk = [&](int c0, float(&wv)[32]) {
                     float y[32];
                     tmem_ld32(tbase + (uint32_t)c0, y);
 #pragma unroll
                     for (int c = 0; c < 32; ++c) y[c] *= wv[c];
-                    if (c0 + 32 < G.bn) {
-#pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            const int b = c0 + 32 + c;
-                            wv[c] = (arow && b < G.cap) ? G.wf[(size_t)b * G.ldw + a_row] : 0.f;
-                        }
-                    }
+                    if (c0 + 64 < G.bn) load_w(wv, c0 + 64);
                     const float s = warp_reduce_scatter32f(y, lane);
                     const int b = c0 + lane;
                     if (b < G.cap)
                         G.dwpart[((size_t)outer * G.nparts + (inner * G.ksplit + un.ks) * 4 + q) * G.cap + b] =
                             (double)s;
+                };
+                for (int c0 = 0; c0 < G.bn; c0 += 64) {
+                    chunk(c0, wa);
+                    if (c0 + 32 < G.bn) chunk(c0 + 32, wb);
                 }
             } else {
                 // Face velocities of this warp's 32 rows, scattered into every
