@@ -171,6 +171,7 @@ struct psf_ctx {
     int vis = 0, tq = 0;
     bool primed = false;
     bool changed = true;  // a setter ran since the last step
+    int sets_since_sort = 0;  // psf_set_particles calls that reused the cell order
     bool have_state = false;
     psf_grid grid{};
     psf_params params{};
@@ -579,7 +580,8 @@ int psf_set_particles(psf_ctx *c, const float *xyzw, int64_t count)
     if (!c || (count > 0 && !xyzw)) return fail(PSF_ERR_INVALID, "null argument");
     if (count < 0 || count > INT32_MAX) return fail(PSF_ERR_INVALID, "bad particle count");
     PSF_CUDA(cudaSetDevice(c->device));
-    if (count != c->d.P) {
+    const bool resized = count != c->d.P;
+    if (resized) {
         PSF_CUDA(cudaStreamSynchronize(c->stream));
         c->drop_graph();
         psf::OrderBufs &o = c->order;
@@ -609,8 +611,15 @@ int psf_set_particles(psf_ctx *c, const float *xyzw, int64_t count)
         c->d.P = count;
     }
     if (count > 0) {
+        // The same particles set again (an end-to-end loop) are still close to
+        // the cell order of the last sort: reuse it, and sort afresh on a new
+        // count and on every RESORT_EVERY-th call.  Results do not depend on the
+        // storage order (respawns are keyed by the caller's index).
+        constexpr int RESORT_EVERY = 8;
+        const bool resort = resized || c->sets_since_sort + 1 >= RESORT_EVERY;
         PSF_CUDA(cudaMemcpyAsync(c->order.staging, xyzw, (size_t)count * 16, cudaMemcpyHostToDevice, c->stream));
-        PSF_CHECK(psf::launch_order_particles(c->d, c->order, c->stream));
+        PSF_CHECK(psf::launch_order_particles(c->d, c->order, c->stream, resort));
+        c->sets_since_sort = resort ? 0 : c->sets_since_sort + 1;
         PSF_CUDA(cudaStreamSynchronize(c->stream));
     }
     return PSF_OK;

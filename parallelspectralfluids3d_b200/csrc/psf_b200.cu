@@ -347,10 +347,15 @@ int sort_particles_temp_bytes(long long P, size_t *bytes)
     return e == cudaSuccess ? PSF_OK : cuda_fail(e, "cub sort sizing");
 }
 
-int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st)
+int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st, bool resort)
 {
     if (d.P == 0) return PSF_OK;
     const unsigned blocks = (unsigned)((d.P + 255) / 256);
+    if (!resort) {  // keep the current order (perm) and only gather the new values into it
+        psf_gather_particles<<<blocks, 256, 0, st>>>(o.staging, d.perm, d.parts, d.P);
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? PSF_OK : cuda_fail(e, "particle gather launch");
+    }
     psf_particle_keys<<<blocks, 256, 0, st>>>(o.staging, d.P, d.grid, o.keys_in, o.idx_in);
     size_t tmp = o.temp_bytes;
     cudaError_t e = cub::DeviceRadixSort::SortPairs(o.temp, tmp, o.keys_in, o.keys_out, o.idx_in,

@@ -111,7 +111,9 @@ int launch_reconstruct(const PlainDev &d, cudaStream_t st, bool after_kernel = t
 int launch_trace(const PlainDev &d, cudaStream_t st, bool after_kernel = true);
 int trace_blocks_per_sm();
 int sort_particles_temp_bytes(long long P, size_t *bytes);
-int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);
+// Put caller-order particles (o.staging) into cell order: a Morton sort that
+// rewrites d.perm, or with `resort` false a gather through the current perm.
+int launch_order_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st, bool resort = true);
 int launch_unorder_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t st);
 
 }  // namespace psf
