@@ -127,6 +127,9 @@ psf::GridDev make_grid_dev(const psf_grid &g)
         const float ext = g.aabb_max[q] - g.aabb_min[q];
         d.shift[q] = g.aabb_min[q] + ext;
     }
+    d.centered = 1;
+    for (int q = 0; q < 3; ++q)
+        if (d.shift[q] != -d.mn[q]) d.centered = 0;
     d.yoff = (uint32_t)((nz + 1) * nx * ny);
     d.xoff = (uint32_t)((nz + 1) * nx * ny + (ny + 1) * nx * nz);
     return d;

@@ -89,7 +89,7 @@ __device__ __forceinline__ unsigned long long cell_key(const GridDev &g, float p
 // face pairs, each second sample of a lerp stored as its difference to the
 // first (mixf(x, y, t) = fma(t, y - x, x) then costs one FMA).
 struct CellCache {
-    unsigned long long key;
+    int kx, ky, kz;        // the cell: floor(2 gi) per axis, clamped to [-1, 2n]
     float oxO, oyO, ozO;   // xO, yO, zO
     float oxM, oyM, ozM;   // xM + 1/2, yM + 1/2, zM + 1/2
     float2 x00, dx10, x01, dx11;  // x faces at (xO, yM|yP, zM|zP), differences along y
@@ -173,20 +173,31 @@ __device__ __forceinline__ float3 interpolate(const CellCache &c, const float3 &
 
 // Velocity at a position; `c` carries the last gathered cell, and the
 // samples are loaded again only when the position lies in another cell.
+// When the box is centred (shift == -mn exactly, as for every domain built
+// here) the reference's index coordinate (shift + p) / h and the weight
+// coordinate (p - mn) / h are the same float, so it is computed once.
 __device__ __forceinline__ float3 velocity_cached(const GridDev &g, const float2 *__restrict__ pairs, float px,
                                                   float py, float pz, CellCache &c, bool &have)
 {
-    int kx, ky, kz;
-    const unsigned long long key = cell_key(g, px, py, pz, kx, ky, kz);
-    if (!have || key != c.key) {
-        c.key = key;
-        gather_cell(g, pairs, kx, ky, kz, c);
-        have = true;
-    }
     float3 gw;
     gw.x = (px - g.mn[0]) * g.inv_h;
     gw.y = (py - g.mn[1]) * g.inv_h;
     gw.z = (pz - g.mn[2]) * g.inv_h;
+    int kx, ky, kz;
+    if (g.centered) {
+        kx = clampi(__float2int_rd(2.0f * gw.x), -1, 2 * g.nx);
+        ky = clampi(__float2int_rd(2.0f * gw.y), -1, 2 * g.ny);
+        kz = clampi(__float2int_rd(2.0f * gw.z), -1, 2 * g.nz);
+    } else {
+        cell_key(g, px, py, pz, kx, ky, kz);
+    }
+    if (!have || kx != c.kx || ky != c.ky || kz != c.kz) {
+        c.kx = kx;
+        c.ky = ky;
+        c.kz = kz;
+        gather_cell(g, pairs, kx, ky, kz, c);
+        have = true;
+    }
     return interpolate(c, gw);
 }
 

@@ -24,6 +24,7 @@ struct GridDev {
     float shift[3];  // aabb min + extent: the reference's index offset (psfsolver.cpp:80)
     uint32_t yoff;   // number of z-faces
     uint32_t xoff;   // number of z- and y-faces
+    int centered;    // shift == -mn on every axis: the index and weight coordinates coincide
 };
 
 struct StateParams {
