@@ -377,7 +377,6 @@ int launch_unorder_particles(const PlainDev &d, const OrderBufs &o, cudaStream_t
 }
 
 // ------------------------------------------------------------- launchers
-// ------------------------------------------------------------- launchers
 int launch_contract_state(const PlainDev &d, cudaStream_t st)
 {
     const int CH = (d.Np + 127) / 128;

@@ -203,6 +203,21 @@ __device__ __forceinline__ float3 velocity_cached(const GridDev &g, const float2
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
+// x / 6 for the RK4 average: the product with r = RN(1/6) and one residual
+// correction by FMA (Markstein's correction step; for a constant divisor see
+// Brisebarre and Muller, "Correctly rounded multiplication by arbitrary
+// precision constants", 2008).  An exhaustive check over all floats finds it
+// equal to the correctly rounded quotient for every |x| >= 2^-120; below
+// that the residual underflows and the result may differ in the last place,
+// which moves no position (|dt x / 6| is then far below an ulp of any
+// coordinate but the smallest).
+__device__ __forceinline__ float div6(float x)
+{
+    const float r = 1.0f / 6.0f;
+    const float q = x * r;
+    return fmaf(fmaf(-q, 6.0f, x), r, q);
+}
+
 // One particle step (psfsolver.cpp:75-224): RK1 or RK4 with the box clamp
 // on every stage, lifetime decrement, and respawn from the counter-based
 // generator keyed by the caller-order index `perm[idx]` when the lifetime ran
@@ -231,9 +246,9 @@ __device__ __forceinline__ float4 advance_particle(float4 p, const GridDev &g, c
             qy = clampf(p.y + dt * k3.y, g.mn[1], g.mx[1]);
             qz = clampf(p.z + dt * k3.z, g.mn[2], g.mx[2]);
             const float3 k4 = velocity_cached(g, u, qx, qy, qz, c, have);
-            v.x = (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x) / 6.f;
-            v.y = (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y) / 6.f;
-            v.z = (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z) / 6.f;
+            v.x = div6(k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
+            v.y = div6(k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
+            v.z = div6(k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
         } else {
             v = velocity_cached(g, u, p.x, p.y, p.z, c, have);
         }
