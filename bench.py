@@ -806,7 +806,7 @@ def run_serve(args, local_rank, rank=0, world=1):
     for spec, n in SERVE_DOMAINS:
         dom = make_domain(spec)
         bases.append(cached_basis(dom, n, cache_dir=basis_cache_for(dom.name, n), device="cuda"))
-    all_reqs = serve_requests(args.serve_seconds, n_max=min(b.n_modes for b in bases))
+    all_reqs = serve_requests(args.serve_seconds, rate=args.serve_rate, n_max=min(b.n_modes for b in bases))
     for i, q in enumerate(all_reqs):
         q["index"] = i
     reqs = replicas.shard(all_reqs, rank, world) if world > 1 else all_reqs
@@ -877,14 +877,18 @@ def run_serve(args, local_rank, rank=0, world=1):
         if rank != 0:
             return None
     out = {"requests": len(all_reqs), "completed": int(lat.size), "arrival_window_s": args.serve_seconds,
-           "gpus": world,
+           "arrival_rate_per_s": args.serve_rate, "gpus": world,
+           # Work offered per second of the arrival window: the served rate
+           # cannot exceed it while the engine keeps up with the arrivals.
+           "offered_instance_steps_per_s": round(sum(q["steps"] for q in all_reqs) / args.serve_seconds, 1),
            "instance_steps": total_steps, "instance_steps_per_s": round(total_steps / (last - first), 1),
            "particle_steps_per_s": round(st["particle_steps"] / (last - first), 1),
            "p50_latency_s": round(float(np.percentile(lat, 50)), 4),
            "p99_latency_s": round(float(np.percentile(lat, 99)), 4),
            "mean_latency_s": round(float(lat.mean()), 4), "makespan_s": round(last - first, 3),
            "wall_s": round(wall, 3), "engine": st,
-           "config": {"slots_per_domain": args.serve_slots, "particle_pool": args.serve_pool,
+           "config": {"arrival_rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
+                      "slots_per_domain": args.serve_slots, "particle_pool": args.serve_pool,
                       "hbm_budget_gb": args.serve_budget_gb, "chunk_steps": args.serve_chunk,
                       "n_range": [64, min(b.n_modes for b in bases)]}}
     # Accuracy of a few served rollouts against the FP64 oracle (w only).
@@ -1086,11 +1090,12 @@ def main():
     ap.add_argument("--ncu-phases", action="store_true",
                     help="profiling driver: run the batched phases as separate launches")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving: length of the arrival window")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--serve-slots", type=int, default=96, help="serving: concurrent rollouts per domain")
     ap.add_argument("--serve-pool", type=int, default=64_000_000, help="serving: particles resident at once")
     ap.add_argument("--serve-budget-gb", type=float, default=16.0, help="serving: device budget of admitted rollouts")
     ap.add_argument("--serve-chunk", type=int, default=8, help="serving: steps between admission rounds")
-    ap.add_argument("--serve-plain-sample", type=int, default=12, help="serving: requests timed on the plain path")
+    ap.add_argument("--serve-plain-sample", type=int, default=32, help="serving: requests timed on the plain path")
     ap.add_argument("--plain-sample", type=int, default=12, help="batched: instances timed on the plain path")
     ap.add_argument("--ncu", type=int, default=0, metavar="S",
                     help="profiling driver: set up the workload, then run S steps kernel by kernel and exit")

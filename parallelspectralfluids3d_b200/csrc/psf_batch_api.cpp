@@ -153,11 +153,22 @@ struct psf_batch {
     std::vector<int64_t> slot_units;  // pool units held by each slot
     int64_t bytes = 0;
     std::vector<void *> allocs;
+    // Reads of slots that the queued steps do not touch (psf::batch_read_frozen):
+    // a second stream and pinned host buffers for one slot's particles.
+    cudaStream_t side = nullptr;
+    float4 *rd_parts = nullptr;
+    int32_t *rd_perm = nullptr;
+    int64_t rd_cap = 0;
+    // Host rows read by copies queued without a synchronisation.
+    std::vector<std::vector<double>> kept_rows;
 
     ~psf_batch()
     {
         drop_graph();
         for (void *p : allocs) cudaFree(p);
+        if (rd_parts) cudaFreeHost(rd_parts);
+        if (rd_perm) cudaFreeHost(rd_perm);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
     void drop_graph()
@@ -750,12 +761,15 @@ int set_one(psf_batch *B, int32_t basis, int32_t slot, const psf_instance_desc *
 }
 
 // After placements: new prefix sums, the contraction partials a fused step
-// starts from, and one synchronisation.
-int finish_placements(psf_batch *B)
+// starts from, and (unless `sync` is false) one synchronisation.
+int finish_placements(psf_batch *B, bool sync = true)
 {
     PSF_CHECK(upload_prefix(B));
     if (B->use_fused) PSF_CHECK(psf::launch_batch_step_tc(B->contract, B->bn_max, B->gemm_ctas, B->stream));
-    PSF_CUDA(cudaStreamSynchronize(B->stream));
+    if (sync) {
+        PSF_CUDA(cudaStreamSynchronize(B->stream));
+        B->kept_rows.clear();
+    }
     return PSF_OK;
 }
 
@@ -867,6 +881,7 @@ int psf_batch_sync(psf_batch *B)
     if (!B) return fail(PSF_ERR_INVALID, "null batch");
     PSF_CUDA(cudaSetDevice(B->device));
     PSF_CUDA(cudaStreamSynchronize(B->stream));
+    B->kept_rows.clear();
     return check_device_error(B);
 }
 
@@ -1015,3 +1030,72 @@ int psf_batch_device_status(psf_batch *B, int32_t *code)
 }
 
 }  // extern "C"
+
+namespace psf {
+
+int batch_place_async(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot,
+                      const psf_instance_desc *const *inst, int32_t *status)
+{
+    if (!B || n < 0 || (n > 0 && (!basis || !slot || !inst || !status))) return fail(PSF_ERR_INVALID, "null argument");
+    PSF_CUDA(cudaSetDevice(B->device));
+    for (int32_t i = 0; i < n; ++i) status[i] = set_one(B, basis[i], slot[i], inst[i], B->kept_rows);
+    return finish_placements(B, false);
+}
+
+int batch_prepare_reads(psf_batch *B)
+{
+    if (!B) return fail(PSF_ERR_INVALID, "null batch");
+    PSF_CUDA(cudaSetDevice(B->device));
+    if (!B->side) PSF_CUDA(cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking));
+    if (B->rd_cap < B->pmax_all) {
+        float4 *parts = nullptr;
+        int32_t *perm = nullptr;
+        PSF_CUDA(cudaHostAlloc((void **)&parts, (size_t)B->pmax_all * 16, cudaHostAllocDefault));
+        cudaError_t e = cudaHostAlloc((void **)&perm, (size_t)B->pmax_all * 4, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaFreeHost(parts);
+            return psf::cuda_fail(e, "cudaHostAlloc");
+        }
+        B->rd_parts = parts;
+        B->rd_perm = perm;
+        B->rd_cap = B->pmax_all;
+    }
+    return PSF_OK;
+}
+
+int batch_read_frozen(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot, double *const *w,
+                      float *const *xyzw)
+{
+    if (!B || n < 0 || (n > 0 && (!basis || !slot || !w || !xyzw))) return fail(PSF_ERR_INVALID, "null argument");
+    if (!B->side || B->rd_cap < B->pmax_all) return fail(PSF_ERR_STATE, "frozen reads are not prepared");
+    PSF_CUDA(cudaSetDevice(B->device));
+    for (int32_t i = 0; i < n; ++i) {
+        int sg = 0;
+        PSF_CHECK(slot_index(B, basis[i], slot[i], &sg));
+        const psf::SlotDev &s = B->slots[(size_t)sg];
+        if (!s.active) return fail(PSF_ERR_STATE, "slot is empty");
+        HostGroup &G = B->groups[(size_t)basis[i]];
+        if (w[i])
+            PSF_CUDA(cudaMemcpyAsync(w[i], G.w + (size_t)slot[i] * G.N, (size_t)s.n_modes * 8, cudaMemcpyDeviceToHost,
+                                     B->side));
+        const int64_t np = s.n_particles;
+        if (xyzw[i] && np > 0) {
+            PSF_CUDA(cudaMemcpyAsync(B->rd_parts, B->pool_parts + s.poff, (size_t)np * 16, cudaMemcpyDeviceToHost,
+                                     B->side));
+            PSF_CUDA(cudaMemcpyAsync(B->rd_perm, B->pool_perm + s.poff, (size_t)np * 4, cudaMemcpyDeviceToHost,
+                                     B->side));
+        }
+        PSF_CUDA(cudaStreamSynchronize(B->side));
+        if (xyzw[i] && np > 0) {
+            float4 *out = reinterpret_cast<float4 *>(xyzw[i]);
+            for (int64_t j = 0; j < np; ++j) {
+                const int32_t d = B->rd_perm[j];
+                if (d < 0 || d >= np) return fail(PSF_ERR_STATE, "particle order index out of range");
+                out[d] = B->rd_parts[j];
+            }
+        }
+    }
+    return PSF_OK;
+}
+
+}  // namespace psf

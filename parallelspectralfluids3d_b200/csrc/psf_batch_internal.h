@@ -119,3 +119,23 @@ int encode_tensor_map(CUtensorMap *map, void *base, int rank, const uint64_t *di
 void split_bf16_host(double x, uint16_t *hi, uint16_t *lo);
 
 }  // namespace psf
+
+// Entry points of psf_batch_api.cpp used by the serving engine
+// (psf_engine.cpp); not part of the C ABI.
+struct psf_batch;
+struct psf_instance_desc;
+namespace psf {
+// psf_batch_set_instances without the closing synchronisation: the copies,
+// orderings and the priming contraction stay queued on the batch's stream.
+// Host rows the copies read are kept until the next psf_batch_sync.
+int batch_place_async(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot,
+                      const psf_instance_desc *const *inst, int32_t *status);
+// Second stream and pinned buffers for batch_read_frozen (once, before use).
+int batch_prepare_reads(psf_batch *B);
+// State and caller-order particles of occupied slots that the work queued on
+// the batch's stream does not step (their step target is reached), read on a
+// second stream while that work runs.  The caller-order scatter runs on the
+// host.
+int batch_read_frozen(psf_batch *B, int32_t n, const int32_t *basis, const int32_t *slot, double *const *w,
+                      float *const *xyzw);
+}  // namespace psf

@@ -1,12 +1,17 @@
 // Serving engine (include/psf_engine.h): continuous batching of rollouts.
 //
-// One worker thread owns a psf_batch.  Each round it admits queued requests
-// (first come first served, skipping requests that do not fit yet) into free
-// slots while the slot count, the particle pool and the device-memory budget
-// allow, launches a chunk of steps for every admitted rollout (a rollout
-// stops on the device at its own step count), and retires finished rollouts
-// by copying their state and particles out and freeing their slot.  Callers
-// submit, poll, wait and collect from any thread.
+// One worker thread owns a psf_batch.  Each round launches a chunk of steps
+// for every admitted rollout (a rollout stops on the device at its own step
+// count) and, while that chunk runs, does the host work of the round:
+//   - it retires the rollouts that reached their step count in the previous
+//     chunk: their slots are no longer stepped, so their state and particles
+//     are read on a second stream beside the running chunk;
+//   - it picks queued requests (first come first served, skipping requests
+//     that do not fit yet) for the slots, particle pool and device-memory
+//     budget that are free, and copies their particles into pinned memory.
+// After the chunk the retired slots are cleared and the picked requests
+// placed (their uploads queued ahead of the next chunk, without waiting).
+// Callers submit, poll, wait and collect from any thread.
 
 #include <cuda_runtime.h>
 
@@ -26,6 +31,7 @@
 
 #include "psf_b200.h"
 #include "psf_batch.h"
+#include "psf_batch_internal.h"
 #include "psf_engine.h"
 #include "psf_internal.h"
 
@@ -43,6 +49,7 @@ struct Request {
     std::vector<float> p_out;
     int status = PSF_OK;
     int slot = -1;
+    const float *src = nullptr;  // pinned copy of `parts` for the placement, if staged
     int64_t remaining = 0;
     int64_t bytes = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
@@ -81,6 +88,13 @@ struct psf_engine {
     std::string fatal_msg;
     std::atomic<bool> stop{false};
     std::thread worker;
+    // Pinned staging of picked requests' particles: two halves used by
+    // alternate rounds; an event marks when the placements reading a half ran.
+    float *arena = nullptr;
+    int64_t arena_floats = 0;  // per half
+    int half = 0;
+    cudaEvent_t half_done[2] = {nullptr, nullptr};
+    bool half_used[2] = {false, false};
 
     double now() const
     {
@@ -93,10 +107,22 @@ struct psf_engine {
         const BasisInfo &b = bases[(size_t)r.basis];
         return (int64_t)r.parts.size() / 4 * 20 + 24 * b.voxels + 16 * (int64_t)b.n_modes;
     }
+    void release()
+    {
+        psf_batch_destroy(batch);
+        batch = nullptr;
+        for (cudaEvent_t &ev : half_done)
+            if (ev) cudaEventDestroy(ev);
+        if (arena) cudaFreeHost(arena);
+        arena = nullptr;
+    }
     void run();
     void finish(const ReqPtr &r, int status);
-    int admit_round();
-    int step_round();
+    std::vector<ReqPtr> pick();
+    int stage(std::vector<ReqPtr> &picked);
+    int place(std::vector<ReqPtr> &picked);
+    int retire(std::vector<ReqPtr> &frozen, std::vector<int32_t> &clear_b, std::vector<int32_t> &clear_s);
+    void fail_all(int rc);
 };
 
 void psf_engine::finish(const ReqPtr &r, int status)
@@ -117,33 +143,68 @@ void psf_engine::finish(const ReqPtr &r, int status)
     cv_done.notify_all();
 }
 
-int psf_engine::admit_round()
+// Queued requests that fit now, in arrival order: a free slot of their basis
+// and room in the budget.  They are moved to `active` with their slot.
+std::vector<ReqPtr> psf_engine::pick()
 {
     std::vector<ReqPtr> picked;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        for (auto it = queue.begin(); it != queue.end();) {
-            const ReqPtr &r = *it;
-            std::vector<int> &fs = free_slots[(size_t)r->basis];
-            if (fs.empty() || (budget > 0 && rollout_bytes + r->bytes > budget)) {
-                st.budget_refusals += 1;
-                ++it;
-                continue;
-            }
-            r->slot = fs.back();
-            fs.pop_back();
-            rollout_bytes += r->bytes;
-            active[(size_t)r->basis][(size_t)r->slot] = r;
-            st.active += 1;
-            st.queued -= 1;
-            picked.push_back(r);
-            it = queue.erase(it);
+    std::lock_guard<std::mutex> lock(mu);
+    size_t free_total = 0;
+    for (const auto &fs : free_slots) free_total += fs.size();
+    for (auto it = queue.begin(); it != queue.end() && free_total > 0;) {
+        const ReqPtr &r = *it;
+        std::vector<int> &fs = free_slots[(size_t)r->basis];
+        if (fs.empty() || (budget > 0 && rollout_bytes + r->bytes > budget)) {
+            st.budget_refusals += 1;
+            ++it;
+            continue;
         }
+        r->slot = fs.back();
+        fs.pop_back();
+        --free_total;
+        rollout_bytes += r->bytes;
+        active[(size_t)r->basis][(size_t)r->slot] = r;
+        st.active += 1;
+        st.queued -= 1;
+        picked.push_back(r);
+        it = queue.erase(it);
     }
+    return picked;
+}
+
+// Copy the picked requests' particles into the pinned half of this round
+// (those that do not fit are placed from their own, pageable, copy).
+int psf_engine::stage(std::vector<ReqPtr> &picked)
+{
+    if (picked.empty() || !arena) return PSF_OK;
+    if (half_used[half]) {
+        cudaError_t e = cudaEventSynchronize(half_done[half]);
+        if (e != cudaSuccess) return psf::cuda_fail(e, "cudaEventSynchronize");
+        half_used[half] = false;
+    }
+    float *base = arena + (size_t)half * (size_t)arena_floats;
+    int64_t used = 0;
+    for (const ReqPtr &r : picked) {
+        r->src = nullptr;
+        const int64_t n = (int64_t)r->parts.size();
+        if (n == 0 || used + n > arena_floats) continue;
+        std::memcpy(base + used, r->parts.data(), (size_t)n * sizeof(float));
+        r->src = base + used;
+        used += n;
+    }
+    return PSF_OK;
+}
+
+// Place the picked requests into their slots.  The uploads, particle
+// orderings and the priming contraction are queued on the batch's stream
+// ahead of the next chunk; nothing waits for them here.
+int psf_engine::place(std::vector<ReqPtr> &picked)
+{
     if (picked.empty()) return PSF_OK;
     std::vector<psf_instance_desc> descs(picked.size());
     std::vector<const psf_instance_desc *> dptr(picked.size());
     std::vector<int32_t> bas(picked.size()), slt(picked.size()), status(picked.size(), PSF_OK);
+    bool staged = false;
     for (size_t i = 0; i < picked.size(); ++i) {
         const ReqPtr &r = picked[i];
         psf_instance_desc &d = descs[i];
@@ -152,7 +213,8 @@ int psf_engine::admit_round()
         d.params = r->params;
         d.w0 = r->w0.data();
         d.forcing = r->force.empty() ? nullptr : r->force.data();
-        d.particles = r->parts.empty() ? nullptr : r->parts.data();
+        d.particles = r->parts.empty() ? nullptr : (r->src ? r->src : r->parts.data());
+        staged |= r->src != nullptr;
         d.n_particles = (int64_t)r->parts.size() / 4;
         d.steps = r->steps;
         dptr[i] = &d;
@@ -160,14 +222,23 @@ int psf_engine::admit_round()
         slt[i] = r->slot;
     }
     const double ta = now();
-    const int rc_all = psf_batch_set_instances(batch, (int32_t)picked.size(), bas.data(), slt.data(), dptr.data(),
-                                               status.data());
+    const int rc_all =
+        psf::batch_place_async(batch, (int32_t)picked.size(), bas.data(), slt.data(), dptr.data(), status.data());
+    if (staged) {
+        void *stream = nullptr;
+        psf_batch_get_stream(batch, &stream);
+        cudaError_t e = cudaEventRecord(half_done[half], (cudaStream_t)stream);
+        if (e != cudaSuccess) return psf::cuda_fail(e, "cudaEventRecord");
+        half_used[half] = true;
+        half ^= 1;
+    }
     {
         std::lock_guard<std::mutex> lock(mu);
         st.admit_s += now() - ta;
     }
     for (size_t i = 0; i < picked.size(); ++i) {
         const ReqPtr &r = picked[i];
+        r->src = nullptr;
         const int rc = rc_all != PSF_OK ? rc_all : status[i];
         if (rc == PSF_ERR_NOMEM) {
             // No contiguous particle range yet: back to the head of the queue.
@@ -191,46 +262,20 @@ int psf_engine::admit_round()
         r->remaining = r->steps;
         st.admitted += 1;
     }
-    return PSF_OK;
+    return rc_all == PSF_ERR_NOMEM ? PSF_OK : rc_all;
 }
 
-int psf_engine::step_round()
+// Read out the rollouts that reached their step count in the previous chunk
+// (their slots are not stepped by the chunk now running) and complete them;
+// their slots are cleared once the running chunk is done.
+int psf_engine::retire(std::vector<ReqPtr> &frozen, std::vector<int32_t> &clear_b, std::vector<int32_t> &clear_s)
 {
-    std::vector<ReqPtr> running;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        for (auto &per : active)
-            for (auto &r : per)
-                if (r && r->remaining > 0) running.push_back(r);
-    }
-    if (running.empty()) return PSF_OK;
-    int64_t most = 0;
-    for (const ReqPtr &r : running) most = std::max(most, r->remaining);
-    const int k = (int)std::min<int64_t>(chunk, most);
-    const double ts = now();
-    int rc = psf_batch_step(batch, k);
-    if (rc == PSF_OK) rc = psf_batch_sync(batch);
-    if (rc != PSF_OK) return rc;
-    const double t_stepped = now();
-    std::vector<ReqPtr> finished;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        st.step_launches += k;
-        st.step_s += t_stepped - ts;
-        for (const ReqPtr &r : running) {
-            const int64_t d = std::min<int64_t>(k, r->remaining);
-            r->remaining -= d;
-            st.instance_steps += d;
-            st.particle_steps += d * ((int64_t)r->parts.size() / 4);
-            if (r->remaining == 0) finished.push_back(r);
-        }
-    }
-    if (finished.empty()) return PSF_OK;
-    std::vector<int32_t> bas(finished.size()), slt(finished.size());
-    std::vector<double *> wp(finished.size());
-    std::vector<float *> pp(finished.size());
-    for (size_t i = 0; i < finished.size(); ++i) {
-        const ReqPtr &r = finished[i];
+    if (frozen.empty()) return PSF_OK;
+    std::vector<int32_t> bas(frozen.size()), slt(frozen.size());
+    std::vector<double *> wp(frozen.size());
+    std::vector<float *> pp(frozen.size());
+    for (size_t i = 0; i < frozen.size(); ++i) {
+        const ReqPtr &r = frozen[i];
         r->w_out.resize((size_t)r->n_modes);
         r->p_out.resize(r->parts.size());
         bas[i] = r->basis;
@@ -239,51 +284,112 @@ int psf_engine::step_round()
         pp[i] = r->p_out.empty() ? nullptr : r->p_out.data();
     }
     const double tr = now();
-    int e = psf_batch_read_instances(batch, (int32_t)finished.size(), bas.data(), slt.data(), wp.data(), pp.data());
-    if (e == PSF_OK) e = psf_batch_clear_instances(batch, (int32_t)finished.size(), bas.data(), slt.data());
+    const int e = psf::batch_read_frozen(batch, (int32_t)frozen.size(), bas.data(), slt.data(), wp.data(), pp.data());
     {
         std::lock_guard<std::mutex> lock(mu);
         st.retire_s += now() - tr;
     }
-    for (const ReqPtr &r : finished) {
+    clear_b.insert(clear_b.end(), bas.begin(), bas.end());
+    clear_s.insert(clear_s.end(), slt.begin(), slt.end());
+    for (const ReqPtr &r : frozen) {
         r->parts.clear();
         r->parts.shrink_to_fit();
         finish(r, e);
     }
-    if (e != PSF_OK) return e;
-    return PSF_OK;
+    return e;
+}
+
+// A device error ends every admitted and queued request.
+void psf_engine::fail_all(int rc)
+{
+    std::vector<ReqPtr> all;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        fatal = rc;
+        fatal_msg = psf_last_error();
+        for (auto &per : active)
+            for (auto &r : per)
+                if (r) all.push_back(r);
+        for (auto &r : queue) all.push_back(r);
+        queue.clear();
+        st.queued = 0;
+    }
+    for (auto &r : all) finish(r, rc);
 }
 
 void psf_engine::run()
 {
+    std::vector<ReqPtr> picked, frozen;
+    std::vector<int32_t> clear_b, clear_s;
     while (!stop.load()) {
-        int rc = admit_round();
-        bool idle = false;
-        {
+        // The device is idle here.  Free the slots retired during the last
+        // chunk, then place the requests picked meanwhile (or pick now).
+        int rc = PSF_OK;
+        if (!clear_b.empty()) {
+            rc = psf_batch_clear_instances(batch, (int32_t)clear_b.size(), clear_b.data(), clear_s.data());
+            clear_b.clear();
+            clear_s.clear();
+        }
+        if (rc == PSF_OK && picked.empty()) {
+            picked = pick();
+            rc = stage(picked);
+        }
+        if (rc == PSF_OK) rc = place(picked);
+        picked.clear();
+        std::vector<ReqPtr> running;
+        if (rc == PSF_OK) {
             std::lock_guard<std::mutex> lock(mu);
-            idle = st.active == 0;
+            for (auto &per : active)
+                for (auto &r : per)
+                    if (r && r->remaining > 0) running.push_back(r);
         }
-        if (idle) {
-            std::unique_lock<std::mutex> lock(mu);
-            cv_work.wait_for(lock, std::chrono::milliseconds(20), [&] { return stop.load() || !queue.empty(); });
-            continue;
-        }
-        if (rc == PSF_OK) rc = step_round();
-        if (rc != PSF_OK) {
-            // A device error ends every admitted and queued request.
-            std::vector<ReqPtr> all;
-            {
-                std::lock_guard<std::mutex> lock(mu);
-                fatal = rc;
-                fatal_msg = psf_last_error();
-                for (auto &per : active)
-                    for (auto &r : per)
-                        if (r) all.push_back(r);
-                for (auto &r : queue) all.push_back(r);
-                queue.clear();
-                st.queued = 0;
+        if (rc == PSF_OK && running.empty()) {
+            if (!frozen.empty()) {
+                rc = retire(frozen, clear_b, clear_s);
+                frozen.clear();
+                if (rc == PSF_OK) continue;
+            } else {
+                std::unique_lock<std::mutex> lock(mu);
+                cv_work.wait_for(lock, std::chrono::milliseconds(20), [&] { return stop.load() || !queue.empty(); });
+                continue;
             }
-            for (auto &r : all) finish(r, rc);
+        }
+        // Launch the next chunk; the rollouts that reach their step count in
+        // it are retired during the chunk after it.
+        int k = 0;
+        const double ts = now();
+        std::vector<ReqPtr> finishing;
+        if (rc == PSF_OK) {
+            int64_t most = 0;
+            for (const ReqPtr &r : running) most = std::max(most, r->remaining);
+            k = (int)std::min<int64_t>(chunk, most);
+            rc = psf_batch_step(batch, k);
+        }
+        if (rc == PSF_OK) {
+            for (const ReqPtr &r : running)
+                if (r->remaining <= k) finishing.push_back(r);
+            rc = retire(frozen, clear_b, clear_s);
+            frozen.clear();
+        }
+        if (rc == PSF_OK) {
+            picked = pick();
+            rc = stage(picked);
+        }
+        if (rc == PSF_OK) rc = psf_batch_sync(batch);
+        if (rc == PSF_OK) {
+            std::lock_guard<std::mutex> lock(mu);
+            st.step_launches += k;
+            st.step_s += now() - ts;
+            for (const ReqPtr &r : running) {
+                const int64_t d = std::min<int64_t>(k, r->remaining);
+                r->remaining -= d;
+                st.instance_steps += d;
+                st.particle_steps += d * ((int64_t)r->parts.size() / 4);
+            }
+            frozen = std::move(finishing);
+        }
+        if (rc != PSF_OK) {
+            fail_all(rc);
             return;
         }
     }
@@ -337,6 +443,21 @@ int psf_engine_create(const psf_engine_config *cfg, int device, psf_engine **out
         for (int s = cfg->slots[i] - 1; s >= 0; --s) e->free_slots[(size_t)i].push_back(s);
         e->active[(size_t)i].resize((size_t)cfg->slots[i]);
     }
+    // Pinned staging for placements (two halves of up to four full-size
+    // requests each), the reads beside a running chunk, and their events.
+    e->arena_floats = 4 * std::max<int64_t>(cfg->max_particles, 1 << 12) * 4;
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce == cudaSuccess)
+        ce = cudaHostAlloc((void **)&e->arena, (size_t)(2 * e->arena_floats) * sizeof(float),
+                           cudaHostAllocPortable);
+    for (int h = 0; h < 2 && ce == cudaSuccess; ++h)
+        ce = cudaEventCreateWithFlags(&e->half_done[h], cudaEventDisableTiming);
+    rc = ce != cudaSuccess ? psf::cuda_fail(ce, "engine staging") : psf::batch_prepare_reads(e->batch);
+    if (rc != PSF_OK) {
+        e->release();
+        delete e;
+        return rc;
+    }
     psf_batch_info bi{};
     psf_batch_info_get(e->batch, &bi);
     e->st.device_bytes = bi.device_bytes;
@@ -348,7 +469,7 @@ int psf_engine_create(const psf_engine_config *cfg, int device, psf_engine **out
             e->run();
         });
     } catch (...) {
-        psf_batch_destroy(e->batch);
+        e->release();
         delete e;
         return fail(PSF_ERR_INVALID, "could not start the engine's worker thread");
     }
@@ -362,7 +483,7 @@ int psf_engine_destroy(psf_engine *e)
     e->stop.store(true);
     e->cv_work.notify_all();
     if (e->worker.joinable()) e->worker.join();
-    psf_batch_destroy(e->batch);
+    e->release();
     delete e;
     return PSF_OK;
 }

@@ -99,6 +99,31 @@ def test_engine_continuous_batching_matches_oracle_and_alone(bases):
         assert np.array_equal(p[:, 3], results[i][1][:, 3])
 
 
+def test_engine_staged_and_unstaged_placements_match_alone(bases):
+    # Six full-size requests picked in one round: the pinned staging holds
+    # four of them, the other two are placed from their own copies.  Each
+    # rollout retires while others still run, read beside the running chunk.
+    qs = [(g, (20 + 3 * i) if g == 0 else (8 + i), 6 + 3 * i, 1024, 20 + i, 0.02, L.PSF_RK4)
+          for i, g in enumerate((0, 1, 0, 1, 0, 1))]
+    with Engine(bases, slots=[3, 3], max_particles=1024, chunk_steps=4) as eng:
+        ids = [_submit(eng, bases, q) for q in qs]
+        eng.drain(120)
+        results = [eng.collect(rid) for rid in ids]
+    for i, q in enumerate(qs):
+        w, p, info = results[i]
+        assert info["status"] == 0
+        with Engine(bases, slots=[1, 1], max_particles=1024, chunk_steps=4) as eng:
+            rid = _submit(eng, bases, q)
+            assert eng.wait(rid, 60)
+            w1, p1, _ = eng.collect(rid)
+        assert rel_err(w, w1) <= MIX_TOL, q
+        assert np.abs(p[:, :3] - p1[:, :3]).max() <= MIX_TOL, q
+        assert np.array_equal(p[:, 3], p1[:, 3]), q
+    ref = _oracle(bases, qs[0])
+    assert rel_err(results[0][0], ref.w) <= W_TOL
+    assert np.abs(results[0][1][:, :3] - ref.pos).max() / bases[0].h <= P_TOL_VOX
+
+
 def test_engine_budget_admits_one_rollout_at_a_time(bases):
     qs = [(0, 37, 6, 300, s, 0.02, L.PSF_RK4) for s in range(4)]
     one = 300 * 20 + 24 * int(np.prod(bases[0].dims)) + 16 * bases[0].n_modes
