@@ -176,6 +176,14 @@ struct psf_ctx {
     bool changed = true;  // a setter ran since the last step
     int sets_since_sort = 0;  // psf_set_particles calls that reused the cell order
     bool have_state = false;
+    // The contraction and reconstruction a lean step begins with, queued by
+    // psf_set_particles on a side stream (they depend on the state only), for
+    // the current ring position and inputs; a later setter drops them.
+    bool eager = false;
+    cudaEvent_t eager_fork = nullptr, eager_done = nullptr;
+    cudaEvent_t h2d_done = nullptr;     // the caller's particles have crossed the bus
+    double *wstage = nullptr;           // pinned copy of the last state set
+    cudaEvent_t wstage_done = nullptr;  // ... and its upload
     psf_grid grid{};
     psf_params params{};
     std::vector<int8_t> sigma;
@@ -188,8 +196,9 @@ struct psf_ctx {
     {
         drop_graph();
         for (void *p : allocs) cudaFree(p);
-        for (cudaEvent_t e : {fork, join[0], join[1], mid, after_b})
+        for (cudaEvent_t e : {fork, join[0], join[1], mid, after_b, eager_fork, eager_done, h2d_done, wstage_done})
             if (e) cudaEventDestroy(e);
+        if (wstage) cudaFreeHost(wstage);
         for (cudaStream_t s : side)
             if (s) cudaStreamDestroy(s);
         if (stream) cudaStreamDestroy(stream);
@@ -283,6 +292,7 @@ static int apply_params(psf_ctx *c, const psf_params &p)
     c->drop_graph();
     c->primed = false;
     c->changed = true;
+    c->eager = false;
     return PSF_OK;
 }
 
@@ -354,6 +364,17 @@ static int launch_step(psf_ctx *c)
 {
     const int kind = c->primed ? STEP_STEADY : (c->changed ? STEP_LEAN : STEP_BOOT);
     const int idx = c->vis * 2 + c->tq;
+    if (kind == STEP_LEAN && c->eager) {
+        // The lean step's contraction and reconstruction are already queued
+        // (psf_set_particles); its tracer remains.
+        PSF_CHECK(psf::launch_trace(c->tracer(c->slot(1), c->tq), c->stream, /*after_kernel=*/false));
+        c->vis = c->slot(1);
+        c->tq = 1 - c->tq;
+        c->primed = false;
+        c->changed = false;
+        c->eager = false;
+        return PSF_OK;
+    }
     if (!c->execs[kind][idx]) {
         for (int v = 0; v < 3; ++v)
             for (int q = 0; q < 2; ++q) {
@@ -446,7 +467,8 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     for (cudaStream_t *s : {&c->side[0], &c->side[1]})
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
-    for (cudaEvent_t *ev : {&c->fork, &c->join[0], &c->join[1], &c->mid, &c->after_b})
+    for (cudaEvent_t *ev : {&c->fork, &c->join[0], &c->join[1], &c->mid, &c->after_b, &c->eager_fork,
+                            &c->eager_done, &c->h2d_done, &c->wstage_done})
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaStreamCreate"));
     c->grid = g;
@@ -488,6 +510,8 @@ int psf_create(const psf_basis_desc *b, const psf_params *params, int device, ps
         c->wbuf[1] = c->wbuf[0] + N;
         c->wbuf[2] = c->wbuf[0] + 2 * N;
         c->ubuf[1] = c->ubuf[0] + F;
+        e = cudaHostAlloc((void **)&c->wstage, (size_t)N * 8, cudaHostAllocDefault);
+        if (e != cudaSuccess) return bail(psf::cuda_fail(e, "cudaHostAlloc"));
         // Per-voxel face pairs read by the tracer, and where each active face goes.
         std::vector<int32_t> hdst;
         psf::face_pair_slots(g, b->active_faces, b->n_active, hdst);
@@ -547,10 +571,15 @@ int psf_set_state(psf_ctx *c, const double *w, int32_t n)
     if (!c || !w) return fail(PSF_ERR_INVALID, "null argument");
     if (n != c->d.N) return fail(PSF_ERR_INVALID, "state length must equal n_modes");
     PSF_CUDA(cudaSetDevice(c->device));
-    PSF_CUDA(cudaMemcpyAsync(c->wbuf[c->vis], w, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
-    PSF_CUDA(cudaStreamSynchronize(c->stream));
+    // Through a pinned copy: the caller's buffer is free on return, and the
+    // call does not wait for the stream.
+    PSF_CUDA(cudaEventSynchronize(c->wstage_done));
+    std::memcpy(c->wstage, w, (size_t)n * 8);
+    PSF_CUDA(cudaMemcpyAsync(c->wbuf[c->vis], c->wstage, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    PSF_CUDA(cudaEventRecord(c->wstage_done, c->stream));
     c->primed = false;
     c->changed = true;
+    c->eager = false;
     c->have_state = true;
     return PSF_OK;
 }
@@ -575,6 +604,7 @@ int psf_set_forcing(psf_ctx *c, const double *f, int32_t n)
     PSF_CUDA(cudaStreamSynchronize(c->stream));
     c->primed = false;
     c->changed = true;
+    c->eager = false;
     return PSF_OK;
 }
 
@@ -620,10 +650,29 @@ int psf_set_particles(psf_ctx *c, const float *xyzw, int64_t count)
         // storage order (respawns are keyed by the caller's index).
         constexpr int RESORT_EVERY = 8;
         const bool resort = resized || c->sets_since_sort + 1 >= RESORT_EVERY;
+        // A lean step comes next (the state changed): its contraction and
+        // reconstruction depend on the state only, so they are queued now on
+        // a side stream and run while the particles cross the bus.
+        const bool eager_now = c->have_state && c->changed && !c->primed && !c->eager;
+        if (eager_now) {
+            PSF_CUDA(cudaEventRecord(c->eager_fork, c->stream));
+            PSF_CUDA(cudaStreamWaitEvent(c->side[0], c->eager_fork, 0));
+            PSF_CHECK(psf::launch_contract_state(c->contraction(c->slot(0), c->slot(1)), c->side[0]));
+            PSF_CHECK(psf::launch_reconstruct(c->reconstruction(c->slot(1), c->tq), c->side[0],
+                                              /*after_kernel=*/true));
+            PSF_CUDA(cudaEventRecord(c->eager_done, c->side[0]));
+        }
         PSF_CUDA(cudaMemcpyAsync(c->order.staging, xyzw, (size_t)count * 16, cudaMemcpyHostToDevice, c->stream));
+        PSF_CUDA(cudaEventRecord(c->h2d_done, c->stream));
         PSF_CHECK(psf::launch_order_particles(c->d, c->order, c->stream, resort));
         c->sets_since_sort = resort ? 0 : c->sets_since_sort + 1;
-        PSF_CUDA(cudaStreamSynchronize(c->stream));
+        if (eager_now) {
+            PSF_CUDA(cudaStreamWaitEvent(c->stream, c->eager_done, 0));
+            c->eager = true;
+        }
+        // Return once the caller's buffer has been read; the ordering (and the
+        // queued lookahead) finish on the stream.
+        PSF_CUDA(cudaEventSynchronize(c->h2d_done));
     }
     return PSF_OK;
 }
@@ -715,6 +764,7 @@ int psf_profile_step(psf_ctx *c, double *kernel_ms, int32_t n)
         c->vis = c->slot(1);
         c->tq = 1 - c->tq;
         c->changed = false;
+        c->eager = false;
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == PSF_OK && e != cudaSuccess) rc = psf::cuda_fail(e, "profiled step");

@@ -210,3 +210,53 @@ def test_resetting_particles_every_step_keeps_results(small_bases):
         outs.append((ctx.get_state(), ctx.get_particles()))
         ctx.close()
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_end_to_end_loop_with_lookahead_at_set_particles(small_bases):
+    """The end-to-end pattern (set state, set particles, step, read both back) queues the lean
+    step's contraction and reconstruction at psf_set_particles.  It must give the same results
+    as stepping on, and a setter between psf_set_particles and the step must still act."""
+    b = small_bases["sphere12x10x9"]
+    w0 = initial_coefficients(b.n_modes, 14)
+    w1 = initial_coefficients(b.n_modes, 15)
+    parts = initial_particles(b, 600, 14)
+    f = np.zeros(b.n_modes)
+    f[2] = 0.3
+    outs = []
+    for loop in (False, True):
+        ctx = Context(b, L.make_params(dt=0.03))
+        ctx.set_state(w0)
+        ctx.set_particles(parts)
+        for _ in range(10):
+            if loop:
+                w, p = ctx.get_state(), ctx.get_particles()
+                ctx.set_state(w)
+                ctx.set_particles(p)
+            ctx.step(1)
+        outs.append((ctx.get_state(), ctx.get_particles(), ctx.get_velocity()))
+        ctx.close()
+    for a, c in zip(outs[0], outs[1]):
+        assert np.array_equal(a, c)
+
+    # Setters after the queued lookahead: a new state, new forcing and time step.
+    ctx = Context(b, L.make_params(dt=0.03))
+    ctx.set_state(w0)
+    ctx.set_particles(parts)
+    u_before = ctx.get_velocity()
+    ctx.set_state(w1)
+    ctx.set_particles(parts)
+    assert np.array_equal(ctx.get_velocity(), u_before)  # the visible field is unchanged until a step
+    ctx.set_state(w0)
+    ctx.step(2)
+    got_a = ctx.get_state()
+    ctx.set_state(w1)
+    ctx.set_particles(parts)
+    ctx.set_forcing(f)
+    ctx.set_params(L.make_params(dt=0.05, flags=L.PSF_FLAG_RENORM | L.PSF_FLAG_FORCING))
+    ctx.step(3)
+    got_b = ctx.get_state()
+    ctx.close()
+    ref_a = O.OracleRollout(b, w0, None, dt=0.03, reconstruct=False).step(2)
+    assert rel_err(got_a, ref_a.w) <= W_TOL
+    ref_b = O.OracleRollout(b, w1, None, dt=0.05, forcing=f, reconstruct=False).step(3)
+    assert rel_err(got_b, ref_b.w) <= W_TOL
