@@ -117,7 +117,9 @@ int psf_destroy(psf_ctx *ctx);
 
 int psf_set_params(psf_ctx *ctx, const psf_params *params);
 
-/* Coefficient state w (AbstractSolver::basisCoeff), FP64 [n]. */
+/* Coefficient state w (AbstractSolver::basisCoeff), FP64 [n].  Setters have
+ * read the caller's buffer when they return; the device work they queue
+ * finishes on the context's stream before any later call's work. */
 int psf_set_state(psf_ctx *ctx, const double *w, int32_t n);
 int psf_get_state(psf_ctx *ctx, double *w, int32_t n);
 
