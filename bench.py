@@ -954,8 +954,8 @@ def run_serve(args, local_rank, rank=0, world=1, shared=None):
 # Serving form of the default line: the configured request mix at 200 req/s
 # over a 15 s window (latency at a load the engine keeps up with; the served
 # rate then equals the offered one), and the same mix arriving at 2000 req/s
-# over 2 s (about 4,000 requests queued at once: the engine's capacity).
-SERVE_FORM_RUNS = (("poisson200_15s", 200.0, 15.0), ("saturated_2000_2s", 2000.0, 2.0))
+# over 4 s (about 8,000 requests queued at once: the engine's capacity).
+SERVE_FORM_RUNS = (("poisson200_15s", 200.0, 15.0), ("saturated_2000_4s", 2000.0, 4.0))
 
 
 def run_serve_form(args, local_rank):
