@@ -954,17 +954,28 @@ def run_serve(args, local_rank, rank=0, world=1, shared=None):
 # Serving form of the default line: the configured request mix at 200 req/s
 # over a 15 s window (latency at a load the engine keeps up with; the served
 # rate then equals the offered one), and the same mix arriving at 2000 req/s
-# over 4 s (about 8,000 requests queued at once: the engine's capacity).
-SERVE_FORM_RUNS = (("poisson200_15s", 200.0, 15.0), ("saturated_2000_4s", 2000.0, 4.0))
+# over 4 s (about 8,000 requests queued at once: the engine's capacity).  The
+# engine's slots and chunk differ: a step's tensor-core work grows with the
+# slots, not with the rollouts in them, so the latency run keeps 96 slots per
+# domain (about 55 rollouts per domain are in flight at 200 req/s) and the
+# capacity run takes 192 with 16-step chunks.
+SERVE_FORM_RUNS = (
+    ("poisson200_15s", 200.0, 15.0, dict(serve_slots=96, serve_pool=64_000_000, serve_budget_gb=16.0,
+                                         serve_chunk=8)),
+    ("saturated_2000_4s", 2000.0, 4.0, dict(serve_slots=192, serve_pool=128_000_000, serve_budget_gb=32.0,
+                                            serve_chunk=16)),
+)
 
 
 def run_serve_form(args, local_rank):
     import copy
 
     shared, out = {}, {}
-    for name, rate, seconds in SERVE_FORM_RUNS:
+    for name, rate, seconds, engine in SERVE_FORM_RUNS:
         a = copy.copy(args)
         a.serve_rate, a.serve_seconds = rate, seconds
+        for k, v in engine.items():
+            setattr(a, k, v)
         t0 = time.perf_counter()
         r = run_serve(a, local_rank, shared=shared)
         r["wall_s"] = round(time.perf_counter() - t0, 1)
@@ -1132,10 +1143,10 @@ def main():
                     help="profiling driver: run the batched phases as separate launches")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving: length of the arrival window")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="serving: Poisson arrival rate (requests/s)")
-    ap.add_argument("--serve-slots", type=int, default=192, help="serving: concurrent rollouts per domain")
-    ap.add_argument("--serve-pool", type=int, default=128_000_000, help="serving: particles resident at once")
-    ap.add_argument("--serve-budget-gb", type=float, default=32.0, help="serving: device budget of admitted rollouts")
-    ap.add_argument("--serve-chunk", type=int, default=16, help="serving: steps between admission rounds")
+    ap.add_argument("--serve-slots", type=int, default=96, help="serving: concurrent rollouts per domain")
+    ap.add_argument("--serve-pool", type=int, default=64_000_000, help="serving: particles resident at once")
+    ap.add_argument("--serve-budget-gb", type=float, default=16.0, help="serving: device budget of admitted rollouts")
+    ap.add_argument("--serve-chunk", type=int, default=8, help="serving: steps between admission rounds")
     ap.add_argument("--serve-plain-sample", type=int, default=32, help="serving: requests timed on the plain path")
     ap.add_argument("--plain-sample", type=int, default=12, help="batched: instances timed on the plain path")
     ap.add_argument("--ncu", type=int, default=0, metavar="S",
