@@ -450,20 +450,25 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) psf_batch_step_tc(const __gri
                     for (int c0 = 0; c0 < G.bn; c0 += 32) chunk(c0, wa);
                 }
             } else {
-                // Face velocities of this warp's 32 rows, scattered into every
-                // slot's per-voxel face pairs (each face lands in its two voxels).
+                // Face velocities of this warp's 32 rows, scattered into the
+                // per-voxel face pairs (each face lands in its two voxels) of
+                // every slot that stepped: the tracer reads no others, so an
+                // empty or finished slot costs no stores.
                 const long long f = (long long)inner * 128 + row;
                 const bool frow = f < G.n_rows;
                 const int32_t d0 = frow ? __ldg(G.pair_dst + 2 * f) : -1;
                 const int32_t d1 = frow ? __ldg(G.pair_dst + 2 * f + 1) : -1;
                 for (int c0 = 0; c0 < G.bn; c0 += 32) {
+                    const int bl = c0 + lane;
+                    const unsigned stepped =
+                        __ballot_sync(0xffffffffu, bl < G.cap && G.slot_of[bl].stepped != 0);
                     float y[32];
                     tmem_ld32(tbase + (uint32_t)c0, y);
-                    if (frow) {
+                    if (frow && stepped) {
 #pragma unroll
                         for (int c = 0; c < 32; ++c) {
                             const int b = c0 + c;
-                            if (b < G.cap) {
+                            if ((stepped >> c) & 1u) {
                                 float *pr = G.pairs + (size_t)b * G.pair_floats;
                                 if (d0 >= 0) pr[d0] = y[c];
                                 if (d1 >= 0) pr[d1] = y[c];

@@ -322,6 +322,7 @@ void fill_gemm_args(psf_batch *B)
         y.pair_dst = G.pair_dst;
         y.pairs = reinterpret_cast<float *>(G.pairs);
         y.pair_floats = 6 * G.V;
+        y.slot_of = B->d_slots + G.slot_base;
         c.r_tiles += y.tiles;
     }
     B->fused = c;

@@ -20,6 +20,8 @@ constexpr int GEMM_MAX_KSPLIT = 4;
 // One basis inside a GEMM launch: A operand (C or Phi) and B operand (the
 // slots' coefficient vectors), both BF16 hi/lo pairs, K-major, 128-byte
 // swizzled by TMA.
+struct SlotDev;
+
 struct alignas(64) GemmGroup {
     CUtensorMap tmA;        // 4D (k inner 64, rows 128, hi/lo 2, outer 1)
     CUtensorMap tmB;        // 3D (k inner 64, bn rows, hi/lo 2)
@@ -40,10 +42,11 @@ struct alignas(64) GemmGroup {
     const int32_t *pair_dst;  // reconstruction: [n_rows][2] float slots in a slot's face pairs
     float *pairs;           // reconstruction: per-voxel face pairs [cap][3V] (float2)
     long long pair_floats;  // 6V: floats per slot in pairs
+    const SlotDev *slot_of; // reconstruction: the group's slots (column b is slot_of[b]); pairs are
+                            // written only for slots that stepped (the tracer reads no others)
 };
 
 struct GroupDev;
-struct SlotDev;
 
 // Arguments of one tensor-core launch: contraction units [0, c_tiles) over
 // g[0 .. n_groups), reconstruction units over g[n_groups .. 2 n_groups).
