@@ -436,6 +436,9 @@ int autotune(psf_batch *B, int need_bn)
     int best_bn = -1, best_grid = B->num_sms, best_ks = 1;
     int rc = PSF_OK;
     bool best_fused = try_fused;
+    // Time the launches as full slots would run them: the reconstruction
+    // writes face pairs only for slots marked as stepped.
+    for (psf::SlotDev &s : B->slots) s.stepped = 1;
     for (int fu = try_fused ? 1 : 0; fu >= 0; --fu)
     for (int v : variants) {
         if (v < need_bn) continue;
@@ -474,7 +477,11 @@ int autotune(psf_batch *B, int need_bn)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (rc != PSF_OK) return rc;
+    for (psf::SlotDev &s : B->slots) s.stepped = 0;
+    if (rc != PSF_OK) {
+        upload_tables(B);
+        return rc;
+    }
     B->bn_max = best_bn;
     B->gemm_ctas = best_grid;
     B->ksplit = best_ks;
