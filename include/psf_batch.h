@@ -112,6 +112,8 @@ int psf_batch_get_stream(psf_batch *b, void **stream);
 /* Per-slot results (synchronising). */
 int psf_batch_get_state(psf_batch *b, int32_t basis, int32_t slot, double *w, int32_t n);
 int psf_batch_get_particles(psf_batch *b, int32_t basis, int32_t slot, float *xyzw, int64_t count);
+/* The face velocities of the slot's state as of its last step (the field its
+ * particles were last traced with; none before a slot's first step). */
 int psf_batch_get_velocity(psf_batch *b, int32_t basis, int32_t slot, float *u, int64_t n_faces);
 int psf_batch_get_steps(psf_batch *b, int32_t basis, int32_t slot, int64_t *steps);
 
